@@ -1,0 +1,240 @@
+/*
+ * lemc.h -- C-ABI boundary of the LaughlinEdge B200 engine (sm_100a).
+ *
+ * Every entry point takes plain pointers and sizes and returns an int status
+ * (LEMC_OK == 0, negative on failure).  Nothing here calls exit(); the C++
+ * drop-in layer (include/modules/*.h) maps a non-zero status back onto the
+ * reference's print-and-exit(1) behaviour.
+ *
+ * Citations name the reference interface each entry point replaces, as
+ * <file within the LaughlinEdge project>:<line>.
+ *
+ * Conventions
+ *  - Complex matrices are row-major, interleaved (re, im) doubles, D x D.
+ *  - Positions are interleaved (x, y) floats, walker-major: xy[(w*N + i)*2 + c].
+ *  - A context owns its device buffers and one CUDA stream; it is not
+ *    thread-safe.  Host buffers are always owned by the caller.
+ */
+#ifndef LEMC_H
+#define LEMC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define LEMC_API __attribute__((visibility("default")))
+#else
+#define LEMC_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define LEMC_OK 0
+#define LEMC_ERR_ARG (-1)       /* invalid argument / configuration          */
+#define LEMC_ERR_CAPACITY (-2)  /* a size exceeds a compiled capacity bound  */
+#define LEMC_ERR_CUDA (-3)      /* a CUDA runtime call failed                */
+#define LEMC_ERR_TIMEOUT (-4)   /* a bounded device wait gave up             */
+#define LEMC_ERR_NUMERIC (-5)   /* non-positive metric / failed factorisation */
+#define LEMC_ERR_STATE (-6)     /* call made in the wrong order              */
+#define LEMC_ERR_NODEVICE (-7)  /* no CUDA device visible                    */
+#define LEMC_ERR_IO (-8)        /* file could not be read or written         */
+
+/* ---- compiled capacity bounds ------------------------------------------ */
+#define LEMC_MAX_DEGREE 24      /* largest power-sum degree k (max Delta L)  */
+#define LEMC_MAX_PARTICLES 1024
+#define LEMC_MAX_GUIDE_PARTS 8  /* distinct parts of a guide partition       */
+
+/* ---- enumerations ------------------------------------------------------ */
+enum lemc_guide {
+  LEMC_GUIDE_LAUGHLIN = 0, /* sample |Psi_m|^2; all rows share one chain       */
+  LEMC_GUIDE_ROW = 1       /* sample |P_a Psi_m|^2 per basis row a (reference) */
+};
+enum lemc_gram_mode {
+  LEMC_GRAM_FP64 = 0,   /* SIMT FP64 accumulation (the exact accumulation)     */
+  LEMC_GRAM_BF16X3 = 1, /* tcgen05 kind::f16, hi/lo split, 3 products         */
+  LEMC_GRAM_BF16X4 = 2, /* tcgen05 kind::f16, hi/lo split, 4 products         */
+  LEMC_GRAM_TF32X3 = 3  /* tcgen05 kind::tf32, hi/lo split, 3 products        */
+};
+/* weight planes recorded per measurement (rows of the record buffer) */
+enum lemc_weight {
+  LEMC_W_ONE = 0,   /* sample weight of the guide (1 for the Laughlin guide)  */
+  LEMC_W_R2 = 1,    /* sum_i |z_i|^2                                           */
+  LEMC_W_R4 = 2,    /* sum_i |z_i|^4                                           */
+  LEMC_W_COS = 3,   /* sum_i cos(l theta_i), l = lemc_config.angular_probe     */
+  LEMC_W_SIN = 4,   /* sum_i sin(l theta_i)                                    */
+  LEMC_W_USER = 5,  /* caller-supplied per-sample potential U(z) (optional)   */
+  LEMC_N_WEIGHTS = 6
+};
+
+/* ---- configuration ------------------------------------------------------ */
+typedef struct lemc_config {
+  int32_t particles;        /* N                                              */
+  int32_t inverse_filling;  /* m (nu = 1/m)                                   */
+  int32_t n_walkers;        /* W, independent Markov chains                  */
+  int32_t lanes_per_walker; /* G in {1,2,4,8,16,32}; 0 = autotuned            */
+  float step_sigma;         /* Gaussian single-particle step (l_B)           */
+  int32_t guide;            /* enum lemc_guide                               */
+  uint64_t seed;            /* Philox-4x32-10 key                            */
+  double radius_scale;      /* R of (z/R)^k in p_k; <= 0 selects sqrt(2 m N) */
+  double init_radius;       /* walkers start uniform in this disk; <=0: sqrt(2mN) */
+  int32_t gram_mode;        /* enum lemc_gram_mode                           */
+  int32_t angular_probe;    /* l of the cos/sin weight planes (0 = off)      */
+  int32_t flush_every;      /* tcgen05 path: K-chunks per FP64 flush (0=auto) */
+  int32_t reserved0;
+} lemc_config;
+
+/* Statistics of a context after lemc_run(). */
+typedef struct lemc_stats {
+  uint64_t sweeps;          /* sweeps executed per walker                     */
+  uint64_t measurements;    /* measurements accumulated per walker            */
+  double acceptance;        /* accepted / proposed single-particle moves       */
+  double tau_int;           /* max integrated autocorrelation time of p_1..p_4 (sweeps) */
+  double tau_int_each[4];   /* per observable |p_k|, k = 1..4                 */
+  double ms_sweep;          /* device time of the sweep kernels (ms, total)   */
+  double ms_basis;          /* device time of the basis build (ms, total)     */
+  double ms_gram;           /* device time of the S/H contraction (ms, total) */
+} lemc_stats;
+
+/* One row of the basis returned by lemc_partitions(): the compressed partition
+ * (part, multiplicity) pairs, in the reference's order.                     */
+typedef struct lemc_partition_row {
+  int32_t dL;        /* angular momentum carried by the partition           */
+  int32_t sector_size;
+  int32_t n_pairs;   /* number of distinct parts                             */
+  int32_t pairs_off; /* offset into the pairs array (2 ints per pair)        */
+} lemc_partition_row;
+
+typedef struct lemc_ctx lemc_ctx;
+
+/* ---- library / device ---------------------------------------------------- */
+LEMC_API int lemc_version(void);
+LEMC_API const char* lemc_status_string(int status);
+/* Number of visible CUDA devices (0 with LEMC_ERR_NODEVICE when none). */
+LEMC_API int lemc_device_count(int* count);
+
+/* ---- basis enumeration (host only) ------------------------------------------
+ * Replaces iparts::integer_partitions (modules/integer_partitions.h:25-93,
+ * modules/partitions/integer_partitions.cu:10-47, :79-140, :199-226): the
+ * partitions of each dL, restricted to at most `particles` parts, compressed
+ * to (part, multiplicity) pairs ordered by ascending multiplicity, listed in
+ * accelerated-ascending generation order.  Call with rows == NULL to size.  */
+LEMC_API int lemc_partitions(int particles, const int32_t* sectors, int n_sectors,
+                    lemc_partition_row* rows, int max_rows, int32_t* pairs,
+                    int max_pair_ints, int* n_rows, int* n_pair_ints,
+                    int* max_degree, int* longest_compressed);
+
+/* ---- context ------------------------------------------------------------
+ * Replaces the per-call set-up of edgeMC::spectrum_compute
+ * (modules/edge_mc/em_spectrum.cu:210-252): device limits, RNG states,
+ * partitions on the device and the capacity checks.                         */
+LEMC_API int lemc_create(const lemc_config* cfg, lemc_ctx** out);
+LEMC_API int lemc_destroy(lemc_ctx* ctx);
+/* Select the angular-momentum sectors whose basis is sampled. */
+LEMC_API int lemc_set_sectors(lemc_ctx* ctx, const int32_t* sectors, int n_sectors);
+/* Guide rows for LEMC_GUIDE_ROW: walker w samples |P_{rows[w % n]}|^2 |Psi|^2,
+ * rows index the basis of the selected sectors.  NULL selects every row. */
+LEMC_API int lemc_set_guide_rows(lemc_ctx* ctx, const int32_t* rows, int n_rows);
+/* Initial walker positions; host_xy == NULL draws them uniformly in the
+ * init disk from the Philox stream (replaces particle_positions_initialize,
+ * modules/edge_mc/em_markovchain.cu:223-263). */
+LEMC_API int lemc_init_walkers(lemc_ctx* ctx, const float* host_xy);
+/* Advance every walker n_sweeps sweeps.  measure != 0 records a sample after
+ * each sweep and accumulates S, H2, H4 (and the row sums for LEMC_GUIDE_ROW).
+ * Replaces burnin + hamiltonian_sampler (em_markovchain.cu:266-334,
+ * em_spectrum.cu:16-136) and the mcmc_* launches (em_spectrum.cu:139-208). */
+LEMC_API int lemc_run(lemc_ctx* ctx, int n_sweeps, int measure);
+/* Zero every accumulator (samples, Gram matrices, series, acceptance). */
+LEMC_API int lemc_reset_accumulators(lemc_ctx* ctx);
+LEMC_API int lemc_synchronize(lemc_ctx* ctx);
+
+/* Basis dimension of a selected sector and of all selected sectors. */
+LEMC_API int lemc_sector_dim(const lemc_ctx* ctx, int sector_index, int* dim);
+LEMC_API int lemc_total_dim(const lemc_ctx* ctx, int* dim);
+
+/* Raw Gram sums of one selected sector, complex D x D interleaved:
+ *   S[a][b]  = sum_samples w1 * conj(v_a) v_b
+ *   H2[a][b] = sum_samples w1 * (sum_i |z_i|^2) conj(v_a) v_b
+ *   H4[a][b] = sum_samples w1 * (sum_i |z_i|^4) conj(v_a) v_b
+ * with v_a = prod_j p_{lambda_j}, p_k = sum_i (z_i / R)^k.  Any output may be
+ * NULL.  *n_samples receives the number of accumulated samples.
+ * Replaces the device->host copy and block averaging of em_spectrum.cu:256-359. */
+LEMC_API int lemc_read_gram(lemc_ctx* ctx, int sector_index, double* S, double* H2,
+                   double* H4, double* n_samples);
+/* Cross-sector Gram with the cos/sin(l theta) planes between two selected
+ * sectors (used by the dynamic structure factor, em_dsf.cu:18-158):
+ *   C[a][b] = sum w1 * (sum_i cos l theta_i) conj(v_a) v_b, a in s1, b in s2. */
+LEMC_API int lemc_read_cross(lemc_ctx* ctx, int sector_a, int sector_b, double* Ccos,
+                    double* Csin, double* Cuser);
+/* Reference-estimator row sums (LEMC_GUIDE_ROW), D x D over all selected rows:
+ *   fg[a][b] = sum_{w in row a} v_b/v_a, gg[a][b] = sum |v_b/v_a|^2 (real),
+ *   fh[a][b] = sum V(z) v_b/v_a with V = omega r^2 + kappa r^4 given here.
+ * Replaces results.fg_ff/gg_ff/fHg_ff (modules/edge_montecarlo.h:15-33). */
+LEMC_API int lemc_read_rows(lemc_ctx* ctx, double omega, double kappa, double* fg,
+                   double* gg, double* fh, double* n_samples_per_row);
+LEMC_API int lemc_read_stats(lemc_ctx* ctx, lemc_stats* st);
+LEMC_API int lemc_read_positions(lemc_ctx* ctx, float* host_xy);
+/* Walker-mean series of Re/Im p_1..p_4 per measurement: series[m*8 + 2(k-1) + c]. */
+LEMC_API int lemc_read_series(lemc_ctx* ctx, double* series, int max_meas, int* n_meas);
+
+/* ---- device-buffer entry points (the hot path, for integrators/tests) ------
+ * All pointers are device pointers; `stream` is a cudaStream_t (NULL = legacy).
+ * One sweep-kernel launch: n_sweeps sweeps of W walkers starting at global
+ * sweep index sweep0, then (measure != 0) one measurement record.
+ *   pos      [W][N] float2, in/out
+ *   rec_p    [K][W] float2, p_k for k = 1..K  (out, measure != 0)
+ *   rec_w    [LEMC_N_WEIGHTS][W] float        (out, measure != 0)
+ *   accepted [W] uint32, accumulated          (in/out, may be NULL)       */
+LEMC_API int lemc_sweep_device(void* pos, int W, int N, int m, float sigma,
+                      uint64_t seed, uint32_t sweep0, int n_sweeps, int K,
+                      double radius_scale, int lanes_per_walker, int measure,
+                      int angular_probe, void* rec_p, void* rec_w,
+                      void* accepted, void* stream);
+/* Basis build: V[row][w] (float, row stride ldv >= W) for the rows of the
+ * selected sectors of ctx, from records rec_p [K][W]. */
+LEMC_API int lemc_basis_device(lemc_ctx* ctx, const void* rec_p, int W, void* V,
+                      int ldv, void* stream);
+/* Accumulate raw Gram sums of ctx's sectors from V (rows x ldv) and rec_w
+ * into the device accumulator of ctx using the given mode. */
+LEMC_API int lemc_gram_device(lemc_ctx* ctx, const void* V, const void* rec_w, int W,
+                     int ldv, int gram_mode, void* stream);
+
+/* ---- FP64 dense tail ----------------------------------------------------
+ * Generalized Hermitian eigenproblem H c = E M c (complex D x D, interleaved).
+ * Eigenvalues ascending; eigenvectors (optional, column j = vector j) are
+ * M-normalised (c^H M c = 1).  M is factorised by Cholesky; when M is not
+ * positive definite the directions with eigenvalues below eps * max are
+ * dropped and *rank reports the kept dimension (evals beyond rank = NaN).
+ * Replaces ges::generalizedEigenproblem::extract_spectrum and
+ * extract_dsf_coefficients (modules/eigensolver/generalized_eigenproblem.cpp:45-95). */
+LEMC_API int lemc_geneig(int D, const double* H, const double* M, double eps,
+                double* evals, double* evecs, int* rank);
+
+/* Normalised matrices from raw Gram sums (reference convention,
+ * em_spectrum.cu:331-335 and the Hermitisation at :383-390):
+ *   M[a][b] = S[a][b] / sqrt(S[a][a] S[b][b]),
+ *   H[a][b] = (omega H2 + kappa H4)[a][b] / sqrt(S[a][a] S[b][b]),
+ * both made Hermitian as (X + X^H)/2.  Any output may be NULL. */
+LEMC_API int lemc_normalise(int D, const double* S, const double* H2, const double* H4,
+                   double omega, double kappa, double* M, double* H);
+
+/* ---- time evolution (FP64) ------------------------------------------------
+ * dC/dt = -i M^-1 (H + f(t) U) C, C(0) = e_0, integrated by the embedded
+ * Cash-Karp RK5(4) pair with error control (abs 1e-10, rel 1e-8) and sampled
+ * at t = s * save_step, s < ceil(end_time / save_step):
+ *   out[s][l] = C^H rho_l C (complex), norms[s] = Re C^H M C.
+ * rho holds L matrices D x D.  f(t, user) is the temporal profile.
+ * Replaces timeEvolution::edgeDensityResponse_compute
+ * (modules/dynamics/dynamics.cpp:24-53, :73-125, :280-290). */
+typedef double (*lemc_profile_fn)(double t, void* user);
+LEMC_API int lemc_evolve(int D, const double* M, const double* H, const double* U,
+                int L, const double* rho, lemc_profile_fn f, void* user,
+                double end_time, double save_step, double* out, double* norms,
+                int* n_save);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LEMC_H */

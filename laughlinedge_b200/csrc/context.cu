@@ -1,0 +1,877 @@
+// C-ABI context: owns the device buffers of one sampling job and drives the
+// sweep -> basis -> Gram pipeline on its own CUDA stream.
+//
+// Reference correspondence: this replaces the host drivers *_compute
+// (modules/edge_mc/em_spectrum.cu:210-422, em_metric.cu:200-392,
+// em_dsf.cu:235-500): where the reference launches one <<<32,128>>> kernel
+// per basis row and reduces per-block partial sums on the host, one context
+// here samples every row of every selected sector in the same launches and
+// keeps FP64 accumulators resident on the device.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "lemc_internal.h"
+#include "partitions.hpp"
+
+using namespace lemc;
+
+namespace {
+
+constexpr int kRowAcc = 13;  // accumulators per (row, column) of the row estimator
+
+#define LEMC_CUDA(call)                                 \
+  do {                                                  \
+    cudaError_t e_ = (call);                            \
+    if (e_ != cudaSuccess) {                            \
+      last_cuda_error() = e_;                           \
+      return LEMC_ERR_CUDA;                             \
+    }                                                   \
+  } while (0)
+
+#define LEMC_TRY(call)      \
+  do {                      \
+    int s_ = (call);        \
+    if (s_ != LEMC_OK) return s_; \
+  } while (0)
+
+cudaError_t& last_cuda_error() {
+  static thread_local cudaError_t e = cudaSuccess;
+  return e;
+}
+
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  int alloc(size_t count) {
+    if (count <= n && p) return LEMC_OK;
+    release();
+    if (count == 0) return LEMC_OK;
+    if (cudaMalloc(&p, count * sizeof(T)) != cudaSuccess) {
+      p = nullptr;
+      n = 0;
+      return LEMC_ERR_CUDA;
+    }
+    n = count;
+    return LEMC_OK;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+};
+
+// Sokal's automatic windowing estimate of the integrated autocorrelation time
+// of one series (A. D. Sokal, "Monte Carlo methods in statistical mechanics",
+// 1997): tau(M) = 1/2 + sum_{t=1..M} rho(t), smallest M with M >= c tau(M).
+double tau_int_sokal(const std::vector<double>& x, double c = 5.0) {
+  const size_t T = x.size();
+  if (T < 8) return NAN;
+  double mean = 0;
+  for (double v : x) mean += v;
+  mean /= T;
+  double c0 = 0;
+  for (double v : x) c0 += (v - mean) * (v - mean);
+  c0 /= T;
+  if (!(c0 > 0)) return NAN;
+  double tau = 0.5;
+  for (size_t t = 1; t < T / 2; ++t) {
+    double ct = 0;
+    for (size_t s = 0; s + t < T; ++s) ct += (x[s] - mean) * (x[s + t] - mean);
+    ct /= T;
+    tau += ct / c0;
+    if (double(t) >= c * tau) return tau;
+  }
+  return tau;
+}
+
+}  // namespace
+
+struct lemc_ctx {
+  lemc_config cfg{};
+  int G = 8;
+  int N = 0, m = 0, W = 0, Wpad = 0;
+  float R = 1.f;
+  cudaStream_t stream = nullptr;
+  bool profile = false;
+
+  // basis
+  bool has_basis = false;
+  Basis basis;
+  int K = 0;              // power sums recorded (>= 4 for the series)
+  int D = 0;              // total rows
+  std::vector<int> sec_row;   // first V row of each sector (Re rows)
+  std::vector<int> sec_goff;  // offset (complex entries) of each sector's D x D block
+  size_t gram_plane = 0;      // sum_s D_s^2
+  std::vector<std::pair<int, int>> cross_pairs;
+  std::vector<size_t> cross_off;
+  size_t cross_plane = 0;
+  int n_gram_jobs = 0, n_cross_jobs = 0;
+  std::vector<int> row_vre, row_vim;  // V rows of each basis row
+
+  // guide rows
+  std::vector<int32_t> walker_row;
+  std::vector<int32_t> row_first;  // walkers of row a: [row_first[a], row_first[a+1])
+
+  // device buffers
+  DevBuf<float2> pos;
+  DevBuf<float2> rec_p;
+  DevBuf<float> rec_w;
+  DevBuf<float> V;
+  DevBuf<uint32_t> accepted;
+  DevBuf<BasisNode> prog;
+  int n_nodes = 0;
+  DevBuf<GramJob> jobs;
+  DevBuf<double> gram;      // 3 planes x gram_plane complex
+  DevBuf<double> cross;     // 3 planes x cross_plane complex
+  DevBuf<double> series;
+  DevBuf<int32_t> d_walker_row, d_guide_pairs, d_guide_npairs, d_row_first, d_row_re, d_row_im;
+  DevBuf<double> rowacc;
+  DevBuf<int> err;
+  // tcgen05 path
+  std::vector<TcTile> tc_tiles;
+  DevBuf<TcTile> d_tc_tiles;
+  DevBuf<double> tc_partials;
+  int tc_splits = 1;
+  DevBuf<int32_t> d_sec_row, d_sec_dim, d_sec_goff;
+
+  bool walkers_ready = false;
+  uint64_t sweeps = 0, meas = 0, sweeps_at_reset = 0;
+  std::vector<double> host_series;  // [meas][8]
+  double ms_sweep = 0, ms_basis = 0, ms_gram = 0;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+};
+
+namespace {
+
+int pick_lanes(int N) {
+  // walker width: aim for about 6-12 particles per lane
+  int G = 1;
+  while (G < 32 && (N + G - 1) / G > 12) G *= 2;
+  while (G > 1 && !sweep_config_ok(G, N)) G /= 2;
+  while (G < 32 && !sweep_config_ok(G, N)) G *= 2;
+  return G;
+}
+
+int build_program(lemc_ctx* c) {
+  // DFS over non-increasing part sequences with sum <= max sector and at most
+  // N parts.  Node value = parent value * p_part.
+  const Basis& B = c->basis;
+  std::map<std::vector<int>, int> key_to_row;
+  for (size_t r = 0; r < B.rows.size(); ++r) {
+    std::vector<int> parts;
+    for (const auto& pp : B.rows[r].pairs)
+      for (int q = 0; q < pp.mult; ++q) parts.push_back(pp.part);
+    std::sort(parts.begin(), parts.end(), std::greater<int>());
+    key_to_row[parts] = int(r);
+  }
+  int smax = 0;
+  bool want0 = false;
+  for (int s : B.sectors) {
+    smax = std::max(smax, s);
+    if (s == 0) want0 = true;
+  }
+  std::vector<BasisNode> prog;
+  if (want0) {
+    auto it = key_to_row.find(std::vector<int>{0});
+    if (it != key_to_row.end())
+      prog.push_back({1, 0, c->row_vre[it->second], c->row_vim[it->second]});
+  }
+  std::vector<int> seq;
+  // iterative DFS
+  struct Frame { int sum, maxpart, next; };
+  std::vector<Frame> st;
+  st.push_back({0, smax, 1});
+  while (!st.empty()) {
+    Frame& f = st.back();
+    const int part = f.next;
+    if (part > f.maxpart || f.sum + part > smax || int(seq.size()) >= c->N) {
+      st.pop_back();
+      if (!seq.empty()) seq.pop_back();
+      continue;
+    }
+    f.next++;
+    seq.push_back(part);
+    std::vector<int> key(seq.begin(), seq.end());
+    std::sort(key.begin(), key.end(), std::greater<int>());
+    auto it = key_to_row.find(key);
+    BasisNode nd{int(seq.size()), part, -1, -1};
+    if (it != key_to_row.end()) {
+      nd.row_re = c->row_vre[it->second];
+      nd.row_im = c->row_vim[it->second];
+    }
+    prog.push_back(nd);
+    st.push_back({f.sum + part, part, 1});
+  }
+  // the DFS above extends sequences with parts <= previous part, i.e. each
+  // multiset exactly once, ordered non-increasingly.
+  c->n_nodes = int(prog.size());
+  LEMC_TRY(c->prog.alloc(prog.size()));
+  LEMC_CUDA(cudaMemcpy(c->prog.p, prog.data(), prog.size() * sizeof(BasisNode),
+                       cudaMemcpyHostToDevice));
+  return LEMC_OK;
+}
+
+int alloc_records(lemc_ctx* c) {
+  LEMC_TRY(c->rec_p.alloc(size_t(c->K) * c->W));
+  LEMC_TRY(c->rec_w.alloc(size_t(LEMC_N_WEIGHTS) * c->Wpad));
+  LEMC_CUDA(cudaMemsetAsync(c->rec_w.p, 0, sizeof(float) * LEMC_N_WEIGHTS * c->Wpad, c->stream));
+  if (c->D > 0) {
+    LEMC_TRY(c->V.alloc(size_t(2) * c->D * c->Wpad));
+    LEMC_CUDA(cudaMemsetAsync(c->V.p, 0, sizeof(float) * 2 * c->D * c->Wpad, c->stream));
+  }
+  return LEMC_OK;
+}
+
+int setup_tc(lemc_ctx* c);
+
+int upload_guide(lemc_ctx* c) {
+  if (c->cfg.guide != LEMC_GUIDE_ROW || !c->has_basis) return LEMC_OK;
+  const int R = int(c->basis.rows.size());
+  std::vector<int32_t> pairs(size_t(R) * 2 * kMaxGuideParts, 0), np(R, 0);
+  for (int r = 0; r < R; ++r) {
+    const auto& pr = c->basis.rows[r].pairs;
+    if (int(pr.size()) > kMaxGuideParts) return LEMC_ERR_CAPACITY;
+    np[r] = int(pr.size());
+    for (size_t q = 0; q < pr.size(); ++q) {
+      // part 0 (the dL = 0 row) is the constant p_0 = N: no guide factor
+      pairs[size_t(r) * 2 * kMaxGuideParts + 2 * q] = pr[q].part;
+      pairs[size_t(r) * 2 * kMaxGuideParts + 2 * q + 1] = pr[q].part > 0 ? pr[q].mult : 0;
+    }
+  }
+  LEMC_TRY(c->d_guide_pairs.alloc(pairs.size()));
+  LEMC_TRY(c->d_guide_npairs.alloc(np.size()));
+  LEMC_CUDA(cudaMemcpy(c->d_guide_pairs.p, pairs.data(), pairs.size() * 4, cudaMemcpyHostToDevice));
+  LEMC_CUDA(cudaMemcpy(c->d_guide_npairs.p, np.data(), np.size() * 4, cudaMemcpyHostToDevice));
+  if (c->walker_row.empty()) {
+    // default: every row, walkers split into contiguous equal blocks
+    std::vector<int32_t> rows(R);
+    for (int r = 0; r < R; ++r) rows[r] = r;
+    c->walker_row.assign(c->W, 0);
+    c->row_first.assign(R + 1, 0);
+    for (int w = 0; w < c->W; ++w) c->walker_row[w] = int32_t((int64_t(w) * R) / c->W);
+  }
+  // row_first from walker_row (walker blocks must be contiguous per row)
+  c->row_first.assign(R + 1, 0);
+  for (int w = 0; w < c->W; ++w) c->row_first[c->walker_row[w] + 1]++;
+  for (int r = 0; r < R; ++r) c->row_first[r + 1] += c->row_first[r];
+  for (int w = 1; w < c->W; ++w)
+    if (c->walker_row[w] < c->walker_row[w - 1]) return LEMC_ERR_ARG;
+  LEMC_TRY(c->d_walker_row.alloc(c->W));
+  LEMC_TRY(c->d_row_first.alloc(R + 1));
+  LEMC_CUDA(cudaMemcpy(c->d_walker_row.p, c->walker_row.data(), 4 * c->W, cudaMemcpyHostToDevice));
+  LEMC_CUDA(cudaMemcpy(c->d_row_first.p, c->row_first.data(), 4 * (R + 1), cudaMemcpyHostToDevice));
+  LEMC_TRY(c->d_row_re.alloc(R));
+  LEMC_TRY(c->d_row_im.alloc(R));
+  LEMC_CUDA(cudaMemcpy(c->d_row_re.p, c->row_vre.data(), 4 * R, cudaMemcpyHostToDevice));
+  LEMC_CUDA(cudaMemcpy(c->d_row_im.p, c->row_vim.data(), 4 * R, cudaMemcpyHostToDevice));
+  LEMC_TRY(c->rowacc.alloc(size_t(R) * R * kRowAcc));
+  LEMC_CUDA(cudaMemset(c->rowacc.p, 0, sizeof(double) * R * R * kRowAcc));
+  return LEMC_OK;
+}
+
+int sweep_once(lemc_ctx* c, int n_sweeps, int measure) {
+  SweepArgs a{};
+  a.pos = c->pos.p;
+  a.rec_p = c->rec_p.p;
+  a.rec_w = c->rec_w.p;
+  a.accepted = c->accepted.p;
+  a.walker_row = c->d_walker_row.p;
+  a.guide_pairs = c->d_guide_pairs.p;
+  a.guide_npairs = c->d_guide_npairs.p;
+  a.err = c->err.p;
+  a.W = c->W;
+  a.N = c->N;
+  a.Npad = c->N;
+  a.m = c->m;
+  a.K = c->K;
+  a.sigma = c->cfg.step_sigma;
+  a.invR = 1.f / c->R;
+  a.seed_lo = uint32_t(c->cfg.seed);
+  a.seed_hi = uint32_t(c->cfg.seed >> 32);
+  a.sweep0 = uint32_t(c->sweeps);
+  a.n_sweeps = n_sweeps;
+  a.measure = measure;
+  a.guide = c->cfg.guide;
+  a.angular_probe = c->cfg.angular_probe;
+  return launch_sweep(a, c->G, c->stream);
+}
+
+int gram_step(lemc_ctx* c, const float* V, const float* rec_w, int W, int mode) {
+  if (c->cfg.guide == LEMC_GUIDE_ROW) {
+    return launch_row_accumulate(V, c->Wpad, rec_w, W, c->d_row_first.p,
+                                 int(c->basis.rows.size()), c->D, c->d_row_re.p, c->d_row_im.p,
+                                 c->rowacc.p, c->stream);
+  }
+  if (mode == LEMC_GRAM_FP64) {
+    const int splits = std::max(1, std::min(64, W / 1024));
+    return launch_gram_simt(V, c->Wpad, rec_w, W, c->jobs.p, c->n_gram_jobs + c->n_cross_jobs,
+                            splits, c->gram.p, c->gram_plane, c->cross.p, c->cross_plane,
+                            c->stream);
+  }
+  if (c->tc_tiles.empty()) LEMC_TRY(setup_tc(c));
+  int s = launch_gram_tc(V, c->Wpad, rec_w, W, c->Wpad, c->d_tc_tiles.p, int(c->tc_tiles.size()),
+                         c->tc_splits, c->tc_partials.p, mode, c->cfg.flush_every, c->err.p,
+                         c->stream);
+  if (s != LEMC_OK) return s;
+  // cross-sector planes (cos/sin/user) are small: FP64 path
+  if (c->n_cross_jobs > 0) {
+    const int splits = std::max(1, std::min(64, W / 1024));
+    s = launch_gram_simt(V, c->Wpad, rec_w, W, c->jobs.p + c->n_gram_jobs, c->n_cross_jobs,
+                         splits, c->gram.p, c->gram_plane, c->cross.p, c->cross_plane, c->stream);
+  }
+  return s;
+}
+
+int setup_tc(lemc_ctx* c) {
+  // 128-row A panels x 32-row B panels over the block-diagonal support of the
+  // per-sector Gram blocks; each tile covers every column it touches.
+  const int rows = 2 * c->D;
+  std::vector<std::pair<int, int>> tiles;
+  for (int i0 = 0; i0 < rows; i0 += 128) {
+    for (int j0 = 0; j0 < rows; j0 += 32) {
+      bool need = false;
+      for (size_t s = 0; s < c->sec_row.size() && !need; ++s) {
+        const int r0 = c->sec_row[s], r1 = r0 + 2 * c->basis.sector_dim[s];
+        if (r0 < i0 + 128 && r1 > i0 && r0 < j0 + 32 && r1 > j0) need = true;
+      }
+      if (need) tiles.push_back({i0, j0});
+    }
+  }
+  int sm = 148;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, dev);
+  const int nt = int(tiles.size());
+  c->tc_splits = std::max(1, std::min((sm + nt - 1) / nt, c->Wpad / 256));
+  c->tc_tiles.clear();
+  for (int s = 0; s < c->tc_splits; ++s)
+    for (int t = 0; t < nt; ++t)
+      c->tc_tiles.push_back({tiles[t].first, tiles[t].second, s, s * nt + t});
+  LEMC_TRY(c->d_tc_tiles.alloc(c->tc_tiles.size()));
+  LEMC_CUDA(cudaMemcpy(c->d_tc_tiles.p, c->tc_tiles.data(), sizeof(TcTile) * c->tc_tiles.size(),
+                       cudaMemcpyHostToDevice));
+  const size_t slot = size_t(128) * 96;
+  LEMC_TRY(c->tc_partials.alloc(slot * c->tc_tiles.size()));
+  LEMC_CUDA(cudaMemsetAsync(c->tc_partials.p, 0, sizeof(double) * slot * c->tc_tiles.size(),
+                            c->stream));
+  std::vector<int32_t> dims(c->basis.sector_dim.begin(), c->basis.sector_dim.end());
+  std::vector<int32_t> goff(c->sec_goff.begin(), c->sec_goff.end());
+  std::vector<int32_t> srow(c->sec_row.begin(), c->sec_row.end());
+  const int ns = int(dims.size());
+  LEMC_TRY(c->d_sec_row.alloc(ns));
+  LEMC_TRY(c->d_sec_dim.alloc(ns));
+  LEMC_TRY(c->d_sec_goff.alloc(ns));
+  LEMC_CUDA(cudaMemcpy(c->d_sec_row.p, srow.data(), 4 * ns, cudaMemcpyHostToDevice));
+  LEMC_CUDA(cudaMemcpy(c->d_sec_dim.p, dims.data(), 4 * ns, cudaMemcpyHostToDevice));
+  LEMC_CUDA(cudaMemcpy(c->d_sec_goff.p, goff.data(), 4 * ns, cudaMemcpyHostToDevice));
+  return LEMC_OK;
+}
+
+// Fold the tcgen05 partial slots into the FP64 Gram planes (idempotent use:
+// partials are zeroed afterwards).
+int flush_tc(lemc_ctx* c) {
+  if (c->tc_tiles.empty()) return LEMC_OK;
+  LEMC_TRY(launch_gram_tc_reduce(c->tc_partials.p, c->d_tc_tiles.p, int(c->tc_tiles.size()),
+                                 c->tc_splits, c->d_sec_row.p, c->d_sec_dim.p, c->d_sec_goff.p,
+                                 int(c->sec_row.size()), c->gram.p, c->stream));
+  LEMC_CUDA(cudaMemsetAsync(c->tc_partials.p, 0,
+                            sizeof(double) * 128 * 96 * c->tc_tiles.size(), c->stream));
+  return LEMC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lemc_version(void) { return 10000; }
+
+const char* lemc_status_string(int s) {
+  switch (s) {
+    case LEMC_OK: return "ok";
+    case LEMC_ERR_ARG: return "invalid argument";
+    case LEMC_ERR_CAPACITY: return "capacity exceeded";
+    case LEMC_ERR_CUDA: return cudaGetErrorString(last_cuda_error());
+    case LEMC_ERR_TIMEOUT: return "bounded device wait timed out";
+    case LEMC_ERR_NUMERIC: return "numerical failure (metric not positive definite)";
+    case LEMC_ERR_STATE: return "call out of order";
+    case LEMC_ERR_NODEVICE: return "no CUDA device";
+    case LEMC_ERR_IO: return "file i/o error";
+    default: return "unknown status";
+  }
+}
+
+int lemc_device_count(int* count) {
+  if (!count) return LEMC_ERR_ARG;
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    *count = 0;
+    return LEMC_ERR_NODEVICE;
+  }
+  *count = n;
+  return LEMC_OK;
+}
+
+int lemc_partitions(int particles, const int32_t* sectors, int n_sectors, lemc_partition_row* rows,
+                    int max_rows, int32_t* pairs, int max_pair_ints, int* n_rows, int* n_pair_ints,
+                    int* max_degree, int* longest) {
+  if (particles <= 0 || n_sectors <= 0 || !sectors) return LEMC_ERR_ARG;
+  std::vector<int> sec(sectors, sectors + n_sectors);
+  for (int s : sec)
+    if (s < 0 || s > 64) return LEMC_ERR_ARG;
+  Basis B = build_basis(particles, sec);
+  int total_pairs = 0;
+  for (const auto& r : B.rows) total_pairs += 2 * int(r.pairs.size());
+  if (n_rows) *n_rows = int(B.rows.size());
+  if (n_pair_ints) *n_pair_ints = total_pairs;
+  if (max_degree) *max_degree = B.max_degree;
+  if (longest) *longest = B.longest;
+  if (!rows) return LEMC_OK;
+  if (max_rows < int(B.rows.size()) || max_pair_ints < total_pairs || !pairs)
+    return LEMC_ERR_CAPACITY;
+  int off = 0;
+  for (size_t i = 0; i < B.rows.size(); ++i) {
+    rows[i].dL = B.rows[i].dL;
+    rows[i].sector_size = B.rows[i].sector_size;
+    rows[i].n_pairs = int(B.rows[i].pairs.size());
+    rows[i].pairs_off = off;
+    for (const auto& pp : B.rows[i].pairs) {
+      pairs[off++] = pp.part;
+      pairs[off++] = pp.mult;
+    }
+  }
+  return LEMC_OK;
+}
+
+int lemc_create(const lemc_config* cfg, lemc_ctx** out) {
+  if (!cfg || !out) return LEMC_ERR_ARG;
+  *out = nullptr;
+  if (cfg->particles < 2 || cfg->particles > LEMC_MAX_PARTICLES) return LEMC_ERR_ARG;
+  if (cfg->inverse_filling < 1 || cfg->n_walkers < 1 || !(cfg->step_sigma > 0.f))
+    return LEMC_ERR_ARG;
+  if (cfg->guide != LEMC_GUIDE_LAUGHLIN && cfg->guide != LEMC_GUIDE_ROW) return LEMC_ERR_ARG;
+  if (cfg->gram_mode < LEMC_GRAM_FP64 || cfg->gram_mode > LEMC_GRAM_TF32X3) return LEMC_ERR_ARG;
+  int ndev = 0;
+  if (lemc_device_count(&ndev) != LEMC_OK) return LEMC_ERR_NODEVICE;
+  lemc_ctx* c = new lemc_ctx();
+  c->cfg = *cfg;
+  c->N = cfg->particles;
+  c->m = cfg->inverse_filling;
+  c->W = cfg->n_walkers;
+  c->Wpad = (c->W + 63) / 64 * 64;
+  const double rcl = std::sqrt(2.0 * c->m * c->N);
+  c->R = float(cfg->radius_scale > 0 ? cfg->radius_scale : rcl);
+  c->profile = cfg->reserved0 != 0;
+  c->G = cfg->lanes_per_walker > 0 ? cfg->lanes_per_walker : pick_lanes(c->N);
+  if (!sweep_config_ok(c->G, c->N)) {
+    delete c;
+    return LEMC_ERR_CAPACITY;
+  }
+  int st = LEMC_OK;
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) st = LEMC_ERR_CUDA;
+  for (auto& e : c->ev)
+    if (st == LEMC_OK && cudaEventCreate(&e) != cudaSuccess) st = LEMC_ERR_CUDA;
+  if (st == LEMC_OK) st = c->pos.alloc(size_t(c->W) * c->N);
+  if (st == LEMC_OK) st = c->accepted.alloc(c->W);
+  if (st == LEMC_OK) st = c->err.alloc(1);
+  if (st == LEMC_OK && cudaMemset(c->accepted.p, 0, 4 * c->W) != cudaSuccess) st = LEMC_ERR_CUDA;
+  if (st == LEMC_OK && cudaMemset(c->err.p, 0, sizeof(int)) != cudaSuccess) st = LEMC_ERR_CUDA;
+  if (st != LEMC_OK) {
+    lemc_destroy(c);
+    return st;
+  }
+  *out = c;
+  return LEMC_OK;
+}
+
+int lemc_destroy(lemc_ctx* c) {
+  if (!c) return LEMC_OK;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  c->pos.release();
+  c->rec_p.release();
+  c->rec_w.release();
+  c->V.release();
+  c->accepted.release();
+  c->prog.release();
+  c->jobs.release();
+  c->gram.release();
+  c->cross.release();
+  c->series.release();
+  c->d_walker_row.release();
+  c->d_guide_pairs.release();
+  c->d_guide_npairs.release();
+  c->d_row_first.release();
+  c->d_row_re.release();
+  c->d_row_im.release();
+  c->rowacc.release();
+  c->err.release();
+  c->d_tc_tiles.release();
+  c->tc_partials.release();
+  c->d_sec_row.release();
+  c->d_sec_dim.release();
+  c->d_sec_goff.release();
+  for (auto& e : c->ev)
+    if (e) cudaEventDestroy(e);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return LEMC_OK;
+}
+
+int lemc_set_sectors(lemc_ctx* c, const int32_t* sectors, int n) {
+  if (!c || !sectors || n <= 0) return LEMC_ERR_ARG;
+  std::vector<int> sec(sectors, sectors + n);
+  for (size_t i = 0; i < sec.size(); ++i) {
+    if (sec[i] < 0 || sec[i] > kMaxDegree) return LEMC_ERR_CAPACITY;
+    for (size_t j = 0; j < i; ++j)
+      if (sec[j] == sec[i]) return LEMC_ERR_ARG;
+  }
+  c->basis = build_basis(c->N, sec);
+  c->has_basis = true;
+  c->D = int(c->basis.rows.size());
+  c->K = std::max(4, c->basis.max_degree);
+  if (c->K > kMaxDegree) return LEMC_ERR_CAPACITY;
+  // V rows: sector s occupies [2*first_s, 2*first_s + 2*D_s): Re rows then Im rows
+  c->sec_row.clear();
+  c->sec_goff.clear();
+  c->row_vre.assign(c->D, 0);
+  c->row_vim.assign(c->D, 0);
+  size_t goff = 0;
+  for (size_t s = 0; s < sec.size(); ++s) {
+    const int first = c->basis.sector_first[s], dim = c->basis.sector_dim[s];
+    c->sec_row.push_back(2 * first);
+    c->sec_goff.push_back(int(goff));
+    goff += size_t(dim) * dim;
+    for (int r = 0; r < dim; ++r) {
+      c->row_vre[first + r] = 2 * first + r;
+      c->row_vim[first + r] = 2 * first + dim + r;
+    }
+  }
+  c->gram_plane = goff;
+  // cross-sector pairs for the angular probe: dL_b - dL_a == l
+  c->cross_pairs.clear();
+  c->cross_off.clear();
+  size_t coff = 0;
+  if (c->cfg.angular_probe > 0) {
+    for (size_t i = 0; i < sec.size(); ++i)
+      for (size_t j = 0; j < sec.size(); ++j)
+        if (sec[j] - sec[i] == c->cfg.angular_probe) {
+          c->cross_pairs.push_back({int(i), int(j)});
+          c->cross_off.push_back(coff);
+          coff += size_t(c->basis.sector_dim[i]) * c->basis.sector_dim[j];
+        }
+  }
+  c->cross_plane = coff;
+  // SIMT jobs
+  std::vector<GramJob> jobs;
+  for (size_t s = 0; s < sec.size(); ++s) {
+    const int dim = c->basis.sector_dim[s];
+    for (int a0 = 0; a0 < dim; a0 += 16)
+      for (int b0 = 0; b0 < dim; b0 += 16)
+        jobs.push_back({c->sec_row[s], dim, c->sec_row[s], dim, a0, b0, 0, c->sec_goff[s]});
+  }
+  c->n_gram_jobs = int(jobs.size());
+  for (size_t q = 0; q < c->cross_pairs.size(); ++q) {
+    const int i = c->cross_pairs[q].first, j = c->cross_pairs[q].second;
+    const int da = c->basis.sector_dim[i], db = c->basis.sector_dim[j];
+    for (int a0 = 0; a0 < da; a0 += 16)
+      for (int b0 = 0; b0 < db; b0 += 16)
+        jobs.push_back({c->sec_row[i], da, c->sec_row[j], db, a0, b0, 1, int(c->cross_off[q])});
+  }
+  c->n_cross_jobs = int(jobs.size()) - c->n_gram_jobs;
+  LEMC_TRY(c->jobs.alloc(jobs.size()));
+  LEMC_CUDA(cudaMemcpy(c->jobs.p, jobs.data(), jobs.size() * sizeof(GramJob), cudaMemcpyHostToDevice));
+  LEMC_TRY(c->gram.alloc(6 * c->gram_plane));
+  LEMC_TRY(c->cross.alloc(6 * std::max<size_t>(1, c->cross_plane)));
+  LEMC_TRY(build_program(c));
+  LEMC_TRY(alloc_records(c));
+  c->tc_tiles.clear();
+  LEMC_TRY(upload_guide(c));
+  return lemc_reset_accumulators(c);
+}
+
+int lemc_set_guide_rows(lemc_ctx* c, const int32_t* rows, int n_rows) {
+  if (!c) return LEMC_ERR_ARG;
+  if (!c->has_basis) return LEMC_ERR_STATE;
+  c->walker_row.clear();
+  if (rows && n_rows > 0) {
+    const int R = int(c->basis.rows.size());
+    c->walker_row.resize(c->W);
+    for (int q = 0; q < n_rows; ++q)
+      if (rows[q] < 0 || rows[q] >= R) return LEMC_ERR_ARG;
+    // contiguous blocks: walker w -> rows[(w * n_rows) / W]
+    for (int w = 0; w < c->W; ++w) c->walker_row[w] = rows[(int64_t(w) * n_rows) / c->W];
+    for (int w = 1; w < c->W; ++w)
+      if (c->walker_row[w] < c->walker_row[w - 1]) return LEMC_ERR_ARG;
+  }
+  return upload_guide(c);
+}
+
+int lemc_init_walkers(lemc_ctx* c, const float* host_xy) {
+  if (!c) return LEMC_ERR_ARG;
+  if (host_xy) {
+    LEMC_CUDA(cudaMemcpyAsync(c->pos.p, host_xy, sizeof(float2) * c->W * c->N,
+                              cudaMemcpyHostToDevice, c->stream));
+  } else {
+    const double r0 = c->cfg.init_radius > 0 ? c->cfg.init_radius : std::sqrt(2.0 * c->m * c->N);
+    LEMC_TRY(launch_init_walkers(c->pos.p, c->W, c->N, float(r0), uint32_t(c->cfg.seed),
+                                 uint32_t(c->cfg.seed >> 32), c->stream));
+  }
+  c->walkers_ready = true;
+  return LEMC_OK;
+}
+
+int lemc_reset_accumulators(lemc_ctx* c) {
+  if (!c) return LEMC_ERR_ARG;
+  if (c->gram.p) LEMC_CUDA(cudaMemsetAsync(c->gram.p, 0, sizeof(double) * c->gram.n, c->stream));
+  if (c->cross.p) LEMC_CUDA(cudaMemsetAsync(c->cross.p, 0, sizeof(double) * c->cross.n, c->stream));
+  if (c->rowacc.p) LEMC_CUDA(cudaMemsetAsync(c->rowacc.p, 0, sizeof(double) * c->rowacc.n, c->stream));
+  if (c->tc_partials.p)
+    LEMC_CUDA(cudaMemsetAsync(c->tc_partials.p, 0, sizeof(double) * c->tc_partials.n, c->stream));
+  if (c->accepted.p) LEMC_CUDA(cudaMemsetAsync(c->accepted.p, 0, 4 * c->W, c->stream));
+  c->meas = 0;
+  c->host_series.clear();
+  c->ms_sweep = c->ms_basis = c->ms_gram = 0;
+  c->sweeps_at_reset = c->sweeps;
+  return LEMC_OK;
+}
+
+int lemc_synchronize(lemc_ctx* c) {
+  if (!c) return LEMC_ERR_ARG;
+  LEMC_CUDA(cudaStreamSynchronize(c->stream));
+  int herr = 0;
+  LEMC_CUDA(cudaMemcpy(&herr, c->err.p, sizeof(int), cudaMemcpyDeviceToHost));
+  if (herr != 0) return LEMC_ERR_TIMEOUT;
+  return LEMC_OK;
+}
+
+int lemc_run(lemc_ctx* c, int n_sweeps, int measure) {
+  if (!c || n_sweeps < 0) return LEMC_ERR_ARG;
+  if (!c->walkers_ready) return LEMC_ERR_STATE;
+  if (measure && !c->has_basis) return LEMC_ERR_STATE;
+  if (n_sweeps == 0) return LEMC_OK;
+  if (!measure) {
+    // burn-in: chunks of sweeps per launch, no records
+    for (int done = 0; done < n_sweeps;) {
+      const int chunk = std::min(64, n_sweeps - done);
+      LEMC_TRY(sweep_once(c, chunk, 0));
+      c->sweeps += chunk;
+      done += chunk;
+    }
+    return LEMC_OK;
+  }
+  LEMC_TRY(c->series.alloc(size_t(8) * n_sweeps));
+  LEMC_CUDA(cudaMemsetAsync(c->series.p, 0, sizeof(double) * 8 * n_sweeps, c->stream));
+  float tms[3] = {0, 0, 0};
+  for (int s = 0; s < n_sweeps; ++s) {
+    if (c->profile) cudaEventRecord(c->ev[0], c->stream);
+    LEMC_TRY(sweep_once(c, 1, 1));
+    c->sweeps += 1;
+    if (c->profile) cudaEventRecord(c->ev[1], c->stream);
+    LEMC_TRY(launch_basis(c->rec_p.p, c->W, c->K, c->N, c->prog.p, c->n_nodes, c->V.p, c->Wpad,
+                          c->series.p + 8 * size_t(s), c->stream));
+    if (c->profile) cudaEventRecord(c->ev[2], c->stream);
+    LEMC_TRY(gram_step(c, c->V.p, c->rec_w.p, c->W, c->cfg.gram_mode));
+    if (c->profile) {
+      cudaEventRecord(c->ev[3], c->stream);
+      LEMC_CUDA(cudaEventSynchronize(c->ev[3]));
+      float t;
+      cudaEventElapsedTime(&t, c->ev[0], c->ev[1]);
+      tms[0] += t;
+      cudaEventElapsedTime(&t, c->ev[1], c->ev[2]);
+      tms[1] += t;
+      cudaEventElapsedTime(&t, c->ev[2], c->ev[3]);
+      tms[2] += t;
+    }
+    c->meas += 1;
+  }
+  c->ms_sweep += tms[0];
+  c->ms_basis += tms[1];
+  c->ms_gram += tms[2];
+  std::vector<double> ser(size_t(8) * n_sweeps);
+  LEMC_CUDA(cudaMemcpyAsync(ser.data(), c->series.p, sizeof(double) * ser.size(),
+                            cudaMemcpyDeviceToHost, c->stream));
+  LEMC_TRY(lemc_synchronize(c));
+  for (double& v : ser) v /= c->W;
+  c->host_series.insert(c->host_series.end(), ser.begin(), ser.end());
+  return LEMC_OK;
+}
+
+int lemc_sector_dim(const lemc_ctx* c, int s, int* dim) {
+  if (!c || !dim) return LEMC_ERR_ARG;
+  if (!c->has_basis) return LEMC_ERR_STATE;
+  if (s < 0 || s >= int(c->basis.sector_dim.size())) return LEMC_ERR_ARG;
+  *dim = c->basis.sector_dim[s];
+  return LEMC_OK;
+}
+
+int lemc_total_dim(const lemc_ctx* c, int* dim) {
+  if (!c || !dim) return LEMC_ERR_ARG;
+  if (!c->has_basis) return LEMC_ERR_STATE;
+  *dim = c->D;
+  return LEMC_OK;
+}
+
+int lemc_read_gram(lemc_ctx* c, int s, double* S, double* H2, double* H4, double* n_samples) {
+  if (!c) return LEMC_ERR_ARG;
+  if (!c->has_basis) return LEMC_ERR_STATE;
+  if (s < 0 || s >= int(c->sec_row.size())) return LEMC_ERR_ARG;
+  if (c->cfg.gram_mode != LEMC_GRAM_FP64) LEMC_TRY(flush_tc(c));
+  const int dim = c->basis.sector_dim[s];
+  const size_t off = 2 * size_t(c->sec_goff[s]);
+  const size_t bytes = sizeof(double) * 2 * dim * dim;
+  double* outs[3] = {S, H2, H4};
+  for (int h = 0; h < 3; ++h)
+    if (outs[h])
+      LEMC_CUDA(cudaMemcpyAsync(outs[h], c->gram.p + 2 * c->gram_plane * h + off, bytes,
+                                cudaMemcpyDeviceToHost, c->stream));
+  LEMC_TRY(lemc_synchronize(c));
+  if (n_samples) *n_samples = double(c->meas) * c->W;
+  return LEMC_OK;
+}
+
+int lemc_read_cross(lemc_ctx* c, int sa, int sb, double* Ccos, double* Csin, double* Cuser) {
+  if (!c) return LEMC_ERR_ARG;
+  if (!c->has_basis) return LEMC_ERR_STATE;
+  for (size_t q = 0; q < c->cross_pairs.size(); ++q) {
+    if (c->cross_pairs[q].first != sa || c->cross_pairs[q].second != sb) continue;
+    const size_t n = size_t(c->basis.sector_dim[sa]) * c->basis.sector_dim[sb];
+    double* outs[3] = {Ccos, Csin, Cuser};
+    for (int h = 0; h < 3; ++h)
+      if (outs[h])
+        LEMC_CUDA(cudaMemcpyAsync(outs[h], c->cross.p + 2 * c->cross_plane * h + 2 * c->cross_off[q],
+                                  sizeof(double) * 2 * n, cudaMemcpyDeviceToHost, c->stream));
+    return lemc_synchronize(c);
+  }
+  return LEMC_ERR_ARG;
+}
+
+int lemc_read_rows(lemc_ctx* c, double omega, double kappa, double* fg, double* gg, double* fh,
+                   double* n_per_row) {
+  if (!c) return LEMC_ERR_ARG;
+  if (!c->has_basis || c->cfg.guide != LEMC_GUIDE_ROW) return LEMC_ERR_STATE;
+  const int D = c->D;
+  std::vector<double> acc(size_t(D) * D * kRowAcc);
+  LEMC_CUDA(cudaMemcpyAsync(acc.data(), c->rowacc.p, sizeof(double) * acc.size(),
+                            cudaMemcpyDeviceToHost, c->stream));
+  LEMC_TRY(lemc_synchronize(c));
+  for (int a = 0; a < D; ++a) {
+    for (int b = 0; b < D; ++b) {
+      const double* q = &acc[(size_t(a) * D + b) * kRowAcc];
+      const size_t o = size_t(a) * D + b;
+      if (fg) { fg[2 * o] = q[0]; fg[2 * o + 1] = q[1]; }
+      if (gg) gg[o] = q[2];
+      if (fh) {
+        fh[2 * o] = omega * q[3] + kappa * q[5];
+        fh[2 * o + 1] = omega * q[4] + kappa * q[6];
+      }
+    }
+    if (n_per_row) n_per_row[a] = double(c->meas) * (c->row_first[a + 1] - c->row_first[a]);
+  }
+  return LEMC_OK;
+}
+
+int lemc_read_stats(lemc_ctx* c, lemc_stats* st) {
+  if (!c || !st) return LEMC_ERR_ARG;
+  std::memset(st, 0, sizeof(*st));
+  std::vector<uint32_t> acc(c->W);
+  LEMC_CUDA(cudaMemcpyAsync(acc.data(), c->accepted.p, 4 * c->W, cudaMemcpyDeviceToHost, c->stream));
+  LEMC_TRY(lemc_synchronize(c));
+  double tot = 0;
+  for (uint32_t a : acc) tot += a;
+  const double swept = double(c->sweeps - c->sweeps_at_reset);
+  st->sweeps = c->sweeps;
+  st->measurements = c->meas;
+  st->acceptance = swept > 0 ? tot / (swept * c->W * c->N) : 0.0;
+  const size_t M = c->host_series.size() / 8;
+  double tmax = NAN;
+  for (int k = 0; k < 4; ++k) {
+    double tk = 0;
+    for (int comp = 0; comp < 2; ++comp) {
+      std::vector<double> x(M);
+      for (size_t i = 0; i < M; ++i) x[i] = c->host_series[8 * i + 2 * k + comp];
+      tk += 0.5 * tau_int_sokal(x);
+    }
+    st->tau_int_each[k] = tk;
+    if (!std::isnan(tk) && (std::isnan(tmax) || tk > tmax)) tmax = tk;
+  }
+  st->tau_int = tmax;
+  st->ms_sweep = c->ms_sweep;
+  st->ms_basis = c->ms_basis;
+  st->ms_gram = c->ms_gram;
+  return LEMC_OK;
+}
+
+int lemc_read_positions(lemc_ctx* c, float* xy) {
+  if (!c || !xy) return LEMC_ERR_ARG;
+  LEMC_CUDA(cudaMemcpyAsync(xy, c->pos.p, sizeof(float2) * c->W * c->N, cudaMemcpyDeviceToHost,
+                            c->stream));
+  return lemc_synchronize(c);
+}
+
+int lemc_read_series(lemc_ctx* c, double* series, int max_meas, int* n_meas) {
+  if (!c) return LEMC_ERR_ARG;
+  const int M = int(c->host_series.size() / 8);
+  if (n_meas) *n_meas = M;
+  if (series) std::memcpy(series, c->host_series.data(), sizeof(double) * 8 * std::min(M, max_meas));
+  return LEMC_OK;
+}
+
+int lemc_sweep_device(void* pos, int W, int N, int m, float sigma, uint64_t seed, uint32_t sweep0,
+                      int n_sweeps, int K, double radius_scale, int G, int measure,
+                      int angular_probe, void* rec_p, void* rec_w, void* accepted, void* stream) {
+  if (!pos || W <= 0 || N < 2 || m < 1 || K < 1 || K > kMaxDegree) return LEMC_ERR_ARG;
+  if (measure && (!rec_p || !rec_w)) return LEMC_ERR_ARG;
+  if (G <= 0) G = pick_lanes(N);
+  if (!sweep_config_ok(G, N)) return LEMC_ERR_CAPACITY;
+  SweepArgs a{};
+  a.pos = static_cast<float2*>(pos);
+  a.rec_p = static_cast<float2*>(rec_p);
+  a.rec_w = static_cast<float*>(rec_w);
+  a.accepted = static_cast<uint32_t*>(accepted);
+  a.W = W;
+  a.N = N;
+  a.Npad = N;
+  a.m = m;
+  a.K = K;
+  a.sigma = sigma;
+  a.invR = float(1.0 / (radius_scale > 0 ? radius_scale : std::sqrt(2.0 * m * N)));
+  a.seed_lo = uint32_t(seed);
+  a.seed_hi = uint32_t(seed >> 32);
+  a.sweep0 = sweep0;
+  a.n_sweeps = n_sweeps;
+  a.measure = measure;
+  a.guide = LEMC_GUIDE_LAUGHLIN;
+  a.angular_probe = angular_probe;
+  return launch_sweep(a, G, static_cast<cudaStream_t>(stream));
+}
+
+int lemc_basis_device(lemc_ctx* c, const void* rec_p, int W, void* V, int ldv, void* stream) {
+  if (!c || !rec_p || !V || W <= 0 || ldv < W) return LEMC_ERR_ARG;
+  if (!c->has_basis) return LEMC_ERR_STATE;
+  return launch_basis(static_cast<const float2*>(rec_p), W, c->K, c->N, c->prog.p, c->n_nodes,
+                      static_cast<float*>(V), ldv, nullptr, static_cast<cudaStream_t>(stream));
+}
+
+int lemc_gram_device(lemc_ctx* c, const void* V, const void* rec_w, int W, int ldv, int mode,
+                     void* stream) {
+  if (!c || !V || !rec_w || W <= 0) return LEMC_ERR_ARG;
+  if (!c->has_basis) return LEMC_ERR_STATE;
+  if (ldv != c->Wpad || W != c->W) return LEMC_ERR_ARG;
+  cudaStream_t saved = c->stream;
+  if (stream) c->stream = static_cast<cudaStream_t>(stream);
+  const int s = gram_step(c, static_cast<const float*>(V), static_cast<const float*>(rec_w), W, mode);
+  c->stream = saved;
+  return s;
+}
+
+}  // extern "C"

@@ -1,0 +1,88 @@
+// Internal declarations shared by the CUDA translation units of liblemc.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/lemc.h"
+
+namespace lemc {
+
+constexpr int kMaxDegree = LEMC_MAX_DEGREE;
+constexpr int kMaxGuideParts = LEMC_MAX_GUIDE_PARTS;
+constexpr int kSweepThreads = 256;  // 8 warps per sweep block
+
+// Arguments of one sweep-kernel launch (device pointers).
+struct SweepArgs {
+  float2* pos;              // [W][N]
+  float2* rec_p;            // [K][W] power sums p_1..p_K (measure != 0)
+  float* rec_w;             // [LEMC_N_WEIGHTS][W] weight planes (measure != 0)
+  uint32_t* accepted;       // [W] accumulated accepted moves (may be null)
+  const int32_t* walker_row;   // [W] guide row (row guide only)
+  const int32_t* guide_pairs;  // [rows][2*kMaxGuideParts] (part, mult)
+  const int32_t* guide_npairs; // [rows]
+  int* err;                 // device error word (may be null)
+  int W, N, Npad, m, K;
+  float sigma, invR;
+  uint32_t seed_lo, seed_hi;
+  uint32_t sweep0;
+  int n_sweeps;
+  int measure;
+  int guide;
+  int angular_probe;
+};
+
+// Node of the depth-first basis program: value[depth] = value[depth-1] * p_part
+// (part 0 stands for p_0 = N); rows < 0 mean "not an output".
+struct BasisNode {
+  int depth;
+  int part;
+  int row_re;
+  int row_im;
+};
+
+// One tile of the SIMT FP64 Gram accumulation.
+struct GramJob {
+  int row_a;   // first V row of the Re part of sector a (Im rows follow at +Da)
+  int Da;
+  int row_b;
+  int Db;
+  int a0, b0;  // tile origin inside the (Da x Db) block
+  int wset;    // 0: {ONE, R2, R4}; 1: {COS, SIN, USER}
+  int out;     // offset (in complex entries) of the (Da x Db) block in the output
+};
+
+int launch_sweep(const SweepArgs& a, int lanes_per_walker, cudaStream_t st);
+size_t sweep_smem_bytes(int lanes_per_walker, int Npad);
+bool sweep_config_ok(int lanes_per_walker, int N);
+
+int launch_init_walkers(float2* pos, int W, int N, float radius, uint32_t seed_lo,
+                        uint32_t seed_hi, cudaStream_t st);
+
+int launch_basis(const float2* rec_p, int W, int K, int N, const BasisNode* prog,
+                 int n_nodes, float* V, int ldv, double* series, cudaStream_t st);
+
+int launch_gram_simt(const float* V, int ldv, const float* rec_w, int W,
+                     const GramJob* jobs, int n_jobs, int n_splits, double* out_set0,
+                     size_t plane0, double* out_set1, size_t plane1, cudaStream_t st);
+
+int launch_row_accumulate(const float* V, int ldv, const float* rec_w, int W,
+                          const int32_t* row_first, int n_rows, int D,
+                          const int32_t* row_re, const int32_t* row_im, double* acc,
+                          cudaStream_t st);
+
+// tcgen05 split-precision Gram (gram_tc.cu).
+struct TcTile {
+  int row0;   // first V row of the 128-row A panel
+  int col0;   // first V row of the 32-row B panel
+  int ksplit; // walker split index
+  int slot;   // FP64 partial slot index
+};
+int launch_gram_tc(const float* V, int ldv, const float* rec_w, int W, int Wpad,
+                   const TcTile* tiles, int n_tiles, int n_splits, double* partials,
+                   int mode, int flush_every, int* err, cudaStream_t st);
+int launch_gram_tc_reduce(const double* partials, const TcTile* tiles, int n_tiles,
+                          int n_splits, const int32_t* sec_row, const int32_t* sec_dim,
+                          const int32_t* sec_goff, int n_sec, double* gram,
+                          cudaStream_t st);
+
+}  // namespace lemc

@@ -1,0 +1,337 @@
+// Metropolis sweep over |P_guide Psi_m|^2 on sm_100a.
+//
+// Target density (z in units of l_B):
+//   |Psi_m|^2 = prod_{i<j} |z_i - z_j|^{2m} exp(-sum_i |z_i|^2 / 2)
+// optionally multiplied by |P_a(z)|^2, P_a = prod_k p_k^{r_k}, for the
+// per-row guide of the reference estimator (reference
+// modules/edge_mc/em_markovchain.cu:266-334 and em_spectrum.cu:49-97).
+//
+// Layout: a walker is a group of G consecutive lanes (G in {1,..,32}; G = 32
+// is one walker per warp).  The walker's coordinates live in shared memory;
+// lane l of the group owns particles j = l, l+G, l+2G, ...  For a move of
+// particle i every lane accumulates the products prod |z'-z_j|^2 and
+// prod |z-z_j|^2 over its particles (one log2 per 8 pairs keeps FP32 in
+// range), the G partial log-ratios are combined with a butterfly of
+// __shfl_xor_sync (all lanes end with bitwise identical sums, hence identical
+// accept decisions), and the owner lane commits the move.
+//
+// Random numbers: one Philox-4x32-10 call per proposed move,
+// counter = {i, sweep, walker, 0}: (u1, u2) -> Box-Muller step, u3 -> the
+// Metropolis test log2(u3) <= log2(acceptance ratio).  Lane l of the group
+// draws the randoms of particle i0 + l of each block of G moves and hands
+// them to the group with three shuffles.
+#include <cuda_runtime.h>
+
+#include "lemc_internal.h"
+#include "lemc_rng.h"
+
+namespace lemc {
+namespace {
+
+constexpr float kLog2e = 1.4426950408889634f;
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// z^k for 1 <= k by binary powering (k < 64).
+__device__ __forceinline__ float2 cpowi(float2 z, int k) {
+  float2 r = make_float2(1.f, 0.f);
+  float2 b = z;
+  while (k) {
+    if (k & 1) r = cmul(r, b);
+    k >>= 1;
+    if (k) b = cmul(b, b);
+  }
+  return r;
+}
+
+__device__ __forceinline__ double2 cpowi_d(float2 z, int k) {
+  double2 r = make_double2(1.0, 0.0);
+  double2 b = make_double2(z.x, z.y);
+  while (k) {
+    if (k & 1) r = make_double2(r.x * b.x - r.y * b.y, r.x * b.y + r.y * b.x);
+    k >>= 1;
+    if (k) b = make_double2(b.x * b.x - b.y * b.y, 2.0 * b.x * b.y);
+  }
+  return r;
+}
+
+template <int G>
+__device__ __forceinline__ float group_sum(float v) {
+#pragma unroll
+  for (int off = G / 2; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off, G);
+  return v;
+}
+
+template <int G>
+__global__ void __launch_bounds__(kSweepThreads)
+sweep_kernel(const SweepArgs a) {
+  constexpr int WPW = 32 / G;           // walkers per warp
+  constexpr int WPB = (kSweepThreads / 32) * WPW;
+  constexpr int GPL = (kMaxGuideParts + G - 1) / G;  // guide slots per lane
+  extern __shared__ float2 sm_pos[];
+
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int gl = lane % G;
+  const int wl = warp * WPW + lane / G;
+  const int w = blockIdx.x * WPB + wl;
+  const bool live = w < a.W;
+  const int N = a.N;
+  float2* zs = sm_pos + (size_t)wl * a.Npad;
+
+  for (int j = gl; j < N; j += G)
+    zs[j] = live ? a.pos[(size_t)w * N + j] : make_float2(3.f * j + 1.f, 0.25f * j);
+  __syncwarp();
+
+  // ---- guide state: the distinct parts of the walker's guide partition ----
+  const bool row_guide = (a.guide == LEMC_GUIDE_ROW);
+  int gk[GPL], gr[GPL];
+  double2 gp[GPL];
+#pragma unroll
+  for (int t = 0; t < GPL; ++t) { gk[t] = 0; gr[t] = 0; gp[t] = make_double2(0.0, 0.0); }
+  if (row_guide && live) {
+    const int row = a.walker_row[w];
+    const int np = a.guide_npairs[row];
+#pragma unroll
+    for (int t = 0; t < GPL; ++t) {
+      const int slot = gl + t * G;
+      if (slot < np) {
+        gk[t] = a.guide_pairs[row * 2 * kMaxGuideParts + 2 * slot];
+        gr[t] = a.guide_pairs[row * 2 * kMaxGuideParts + 2 * slot + 1];
+      }
+    }
+  }
+
+  const float sigma = a.sigma;
+  const float invR = a.invR;
+  const float mf = float(a.m);
+  uint32_t nacc = 0;
+
+  for (int s = 0; s < a.n_sweeps; ++s) {
+    const uint32_t sweep = a.sweep0 + uint32_t(s);
+    // refresh the guide power sums from the positions (bounds FP drift)
+    if (row_guide) {
+#pragma unroll
+      for (int t = 0; t < GPL; ++t) {
+        if (gk[t] > 0) {
+          double2 acc = make_double2(0.0, 0.0);
+          for (int j = 0; j < N; ++j) {
+            const float2 z = zs[j];
+            const double2 v = cpowi_d(make_float2(z.x * invR, z.y * invR), gk[t]);
+            acc.x += v.x;
+            acc.y += v.y;
+          }
+          gp[t] = acc;
+        }
+      }
+    }
+
+    for (int i0 = 0; i0 < N; i0 += G) {
+      // lane gl draws the randoms of particle i0 + gl
+      float pzx = 0.f, pzy = 0.f, plu = 0.f;
+      {
+        const int i = i0 + gl;
+        if (i < N) {
+          const U4 r = philox4x32_10(U4{uint32_t(i), sweep, uint32_t(w), kTagMove}, a.seed_lo,
+                                     a.seed_hi);
+          const float u1 = u01(r.x), u2 = u01(r.y), u3 = u01(r.z);
+          const float rad = sqrtf(-2.f * logf(u1));
+          float sn, cs;
+          sincospif(2.f * u2, &sn, &cs);
+          const float2 zi = zs[i];
+          pzx = zi.x + sigma * (rad * cs);
+          pzy = zi.y + sigma * (rad * sn);
+          plu = log2f(u3);
+        }
+      }
+      const int nb = min(G, N - i0);
+      for (int b = 0; b < nb; ++b) {
+        const int im = i0 + b;
+        const float2 zo = zs[im];
+        const float xn = __shfl_sync(0xffffffffu, pzx, b, G);
+        const float yn = __shfl_sync(0xffffffffu, pzy, b, G);
+        const float lu = __shfl_sync(0xffffffffu, plu, b, G);
+
+        // Jastrow log2-ratio over this lane's particles
+        float part = 0.f;
+        float num = 1.f, den = 1.f;
+        int cnt = 0;
+        for (int j = gl; j < N; j += G) {
+          if (j != im) {
+            const float2 zj = zs[j];
+            const float dx = xn - zj.x, dy = yn - zj.y;
+            const float ex = zo.x - zj.x, ey = zo.y - zj.y;
+            num *= fmaf(dx, dx, dy * dy);
+            den *= fmaf(ex, ex, ey * ey);
+            if (++cnt == 8) {
+              part += __log2f(num) - __log2f(den);
+              num = 1.f;
+              den = 1.f;
+              cnt = 0;
+            }
+          }
+        }
+        part += __log2f(num) - __log2f(den);
+        part *= mf;
+
+        // guide polynomial ratio |P_a(z')/P_a(z)|^2 (row guide)
+        double2 gnew[GPL];
+        if (row_guide) {
+          const float2 wo = make_float2(zo.x * invR, zo.y * invR);
+          const float2 wn = make_float2(xn * invR, yn * invR);
+#pragma unroll
+          for (int t = 0; t < GPL; ++t) {
+            gnew[t] = gp[t];
+            if (gk[t] > 0) {
+              const double2 po = cpowi_d(wo, gk[t]);
+              const double2 pn = cpowi_d(wn, gk[t]);
+              gnew[t].x = gp[t].x - po.x + pn.x;
+              gnew[t].y = gp[t].y - po.y + pn.y;
+              const double n1 = gnew[t].x * gnew[t].x + gnew[t].y * gnew[t].y;
+              const double n0 = gp[t].x * gp[t].x + gp[t].y * gp[t].y;
+              part += float(gr[t]) * (__log2f(float(n1)) - __log2f(float(n0)));
+            }
+          }
+        }
+
+        const float tot = group_sum<G>(part);
+        const float gauss = (fmaf(zo.x, zo.x, zo.y * zo.y) - fmaf(xn, xn, yn * yn)) * (0.5f * kLog2e);
+        const bool accept = (tot + gauss) >= lu;
+        if (accept) {
+          if (gl == b) zs[im] = make_float2(xn, yn);
+          ++nacc;
+          if (row_guide) {
+#pragma unroll
+            for (int t = 0; t < GPL; ++t) gp[t] = gnew[t];
+          }
+        }
+        __syncwarp();
+      }
+    }
+  }
+
+  if (live) {
+    for (int j = gl; j < N; j += G) a.pos[(size_t)w * N + j] = zs[j];
+    if (gl == 0 && a.accepted) a.accepted[w] += nacc;
+  }
+
+  if (!a.measure) return;
+
+  // ---- measurement record: p_k = sum_i (z_i / R)^k, k = 1..K, and weights ----
+  float2 acc[kMaxDegree];
+#pragma unroll
+  for (int k = 0; k < kMaxDegree; ++k) acc[k] = make_float2(0.f, 0.f);
+  float h2 = 0.f, h4 = 0.f, hc = 0.f, hs = 0.f;
+  const int K = a.K;
+  for (int j = gl; j < N; j += G) {
+    const float2 z = zs[j];
+    const float2 wv = make_float2(z.x * invR, z.y * invR);
+    float2 pw = wv;
+#pragma unroll
+    for (int k = 0; k < kMaxDegree; ++k) {
+      if (k < K) {
+        acc[k].x += pw.x;
+        acc[k].y += pw.y;
+        pw = cmul(pw, wv);
+      }
+    }
+    const float r2 = fmaf(z.x, z.x, z.y * z.y);
+    h2 += r2;
+    h4 = fmaf(r2, r2, h4);
+    if (a.angular_probe > 0) {
+      const float rinv = rsqrtf(r2);
+      const float2 u = cpowi(make_float2(z.x * rinv, z.y * rinv), a.angular_probe);
+      hc += u.x;
+      hs += u.y;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < kMaxDegree; ++k) {
+    if (k < K) {
+      acc[k].x = group_sum<G>(acc[k].x);
+      acc[k].y = group_sum<G>(acc[k].y);
+    }
+  }
+  h2 = group_sum<G>(h2);
+  h4 = group_sum<G>(h4);
+  hc = group_sum<G>(hc);
+  hs = group_sum<G>(hs);
+  if (!live) return;
+#pragma unroll
+  for (int k = 0; k < kMaxDegree; ++k)
+    if (k < K && (k % G) == gl) a.rec_p[(size_t)k * a.W + w] = acc[k];
+  if (gl == 0) {
+    const size_t W = a.W;
+    a.rec_w[LEMC_W_ONE * W + w] = 1.f;
+    a.rec_w[LEMC_W_R2 * W + w] = h2;
+    a.rec_w[LEMC_W_R4 * W + w] = h4;
+    a.rec_w[LEMC_W_COS * W + w] = hc;
+    a.rec_w[LEMC_W_SIN * W + w] = hs;
+    a.rec_w[LEMC_W_USER * W + w] = 0.f;
+  }
+}
+
+// Uniform initial positions in a disk, Philox counter {i, 0, w, 1}.
+__global__ void init_walkers_kernel(float2* pos, int W, int N, float radius, uint32_t k0,
+                                    uint32_t k1) {
+  const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (t >= (size_t)W * N) return;
+  const uint32_t w = uint32_t(t / N), i = uint32_t(t % N);
+  const U4 r = philox4x32_10(U4{i, 0u, w, kTagInit}, k0, k1);
+  const float rho = radius * sqrtf(u01(r.x));
+  float sn, cs;
+  sincospif(2.f * u01(r.y), &sn, &cs);
+  pos[t] = make_float2(rho * cs, rho * sn);
+}
+
+template <int G>
+int launch_g(const SweepArgs& a, cudaStream_t st) {
+  constexpr int WPB = (kSweepThreads / 32) * (32 / G);
+  const size_t smem = size_t(WPB) * a.Npad * sizeof(float2);
+  if (smem > 227 * 1024) return LEMC_ERR_CAPACITY;
+  if (smem > 48 * 1024) {
+    if (cudaFuncSetAttribute(sweep_kernel<G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(smem)) != cudaSuccess)
+      return LEMC_ERR_CUDA;
+  }
+  const int blocks = (a.W + WPB - 1) / WPB;
+  sweep_kernel<G><<<blocks, kSweepThreads, smem, st>>>(a);
+  return cudaPeekAtLastError() == cudaSuccess ? LEMC_OK : LEMC_ERR_CUDA;
+}
+
+}  // namespace
+
+size_t sweep_smem_bytes(int G, int Npad) {
+  return size_t((kSweepThreads / 32) * (32 / G)) * Npad * sizeof(float2);
+}
+
+bool sweep_config_ok(int G, int N) {
+  if (G != 1 && G != 2 && G != 4 && G != 8 && G != 16 && G != 32) return false;
+  return sweep_smem_bytes(G, N) <= 227 * 1024;
+}
+
+int launch_sweep(const SweepArgs& a, int G, cudaStream_t st) {
+  if (a.K > kMaxDegree || a.N <= 1 || a.W <= 0) return LEMC_ERR_ARG;
+  switch (G) {
+    case 1: return launch_g<1>(a, st);
+    case 2: return launch_g<2>(a, st);
+    case 4: return launch_g<4>(a, st);
+    case 8: return launch_g<8>(a, st);
+    case 16: return launch_g<16>(a, st);
+    case 32: return launch_g<32>(a, st);
+    default: return LEMC_ERR_ARG;
+  }
+}
+
+int launch_init_walkers(float2* pos, int W, int N, float radius, uint32_t k0, uint32_t k1,
+                        cudaStream_t st) {
+  const size_t n = size_t(W) * N;
+  const int threads = 256;
+  const unsigned blocks = unsigned((n + threads - 1) / threads);
+  init_walkers_kernel<<<blocks, threads, 0, st>>>(pos, W, N, radius, k0, k1);
+  return cudaPeekAtLastError() == cudaSuccess ? LEMC_OK : LEMC_ERR_CUDA;
+}
+
+}  // namespace lemc

@@ -1,0 +1,204 @@
+"""Python face of the C-ABI: the sampling context and the FP64 dense tail.
+
+Names mirror the reference's host API (modules/edge_montecarlo.h:199-236):
+:func:`spectrum_compute`, :func:`metric_compute` and :func:`dsf_compute` run the
+same estimators the C++ drop-in layer runs, through ``liblemc.so``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, dptr, fptr, i32ptr
+
+
+def partitions(particles: int, sectors):
+    """Basis rows in reference order: list of (dL, [(part, mult), ...])."""
+    lib = _lib.load()
+    sec = np.ascontiguousarray(sectors, dtype=np.int32)
+    n_rows, n_ints, maxdeg, longest = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+    check(lib.lemc_partitions(particles, i32ptr(sec), len(sec), None, 0, None, 0,
+                              C.byref(n_rows), C.byref(n_ints), C.byref(maxdeg), C.byref(longest)),
+          "lemc_partitions")
+    rows = (_lib.PartitionRow * max(1, n_rows.value))()
+    pairs = np.zeros(max(1, n_ints.value), dtype=np.int32)
+    check(lib.lemc_partitions(particles, i32ptr(sec), len(sec), rows, n_rows.value, i32ptr(pairs),
+                              len(pairs), C.byref(n_rows), C.byref(n_ints), None, None),
+          "lemc_partitions")
+    out = []
+    for r in rows[: n_rows.value]:
+        pr = [(int(pairs[r.pairs_off + 2 * q]), int(pairs[r.pairs_off + 2 * q + 1]))
+              for q in range(r.n_pairs)]
+        out.append((int(r.dL), pr))
+    return out, maxdeg.value, longest.value
+
+
+def _cplx(buf: np.ndarray, D: int) -> np.ndarray:
+    return buf.view(np.complex128).reshape(D, D)
+
+
+def geneig(H: np.ndarray, M: np.ndarray, eps: float = 1e-12, vectors: bool = False):
+    """Generalized Hermitian eigenproblem H c = E M c (FP64, liblemc)."""
+    lib = _lib.load()
+    D = H.shape[0]
+    Hb = np.ascontiguousarray(H, dtype=np.complex128).view(np.float64)
+    Mb = np.ascontiguousarray(M, dtype=np.complex128).view(np.float64)
+    ev = np.zeros(D)
+    vec = np.zeros(2 * D * D) if vectors else None
+    rank = C.c_int()
+    check(lib.lemc_geneig(D, dptr(Hb.ravel()), dptr(Mb.ravel()), eps, dptr(ev),
+                          dptr(vec) if vectors else None, C.byref(rank)), "lemc_geneig")
+    if vectors:
+        return ev, _cplx(vec, D), rank.value
+    return ev
+
+
+def normalise(S, H2=None, H4=None, omega=0.0, kappa=0.0):
+    """Reference normalisation M = S/sqrt(S_aa S_bb), H = (w H2 + k H4)/sqrt(..), Hermitised."""
+    lib = _lib.load()
+    D = S.shape[0]
+    f = lambda X: None if X is None else dptr(np.ascontiguousarray(X, dtype=np.complex128).view(np.float64).ravel())
+    keep = [np.ascontiguousarray(X, dtype=np.complex128) for X in (S, H2, H4) if X is not None]
+    Mo = np.zeros(2 * D * D)
+    Ho = np.zeros(2 * D * D)
+    check(lib.lemc_normalise(D, f(S), f(H2), f(H4), omega, kappa, dptr(Mo), dptr(Ho)), "lemc_normalise")
+    del keep
+    return _cplx(Mo, D), _cplx(Ho, D)
+
+
+def evolve(M, H, U, rho, profile, end_time, save_step):
+    """FP64 edge-basis time evolution; returns (times, <rho_l>(t) [n_save, L], norms)."""
+    lib = _lib.load()
+    D = M.shape[0]
+    rho = [np.ascontiguousarray(r, dtype=np.complex128) for r in rho]
+    L = len(rho)
+    rb = np.ascontiguousarray(np.stack(rho) if L else np.zeros((1, D, D), complex)).view(np.float64).ravel()
+    ns = int(math.ceil(end_time / save_step))
+    out = np.zeros(2 * ns * max(L, 1))
+    norms = np.zeros(ns)
+    n_save = C.c_int()
+    cb = _lib.PROFILE_FN(lambda t, u: float(profile(t)))
+    a = [np.ascontiguousarray(X, dtype=np.complex128).view(np.float64).ravel() for X in (M, H, U)]
+    check(lib.lemc_evolve(D, dptr(a[0]), dptr(a[1]), dptr(a[2]), L, dptr(rb), cb, None,
+                          end_time, save_step, dptr(out), dptr(norms), C.byref(n_save)), "lemc_evolve")
+    times = np.arange(ns) * save_step
+    return times, out.view(np.complex128).reshape(ns, max(L, 1))[:, :L], norms
+
+
+@dataclass
+class SamplerConfig:
+    particles: int
+    inverse_filling: int
+    n_walkers: int
+    step_sigma: float = 0.3
+    seed: int = 42
+    lanes_per_walker: int = 0
+    guide: int = _lib.GUIDE_LAUGHLIN
+    radius_scale: float = 0.0
+    init_radius: float = 0.0
+    gram_mode: int = _lib.GRAM_FP64
+    angular_probe: int = 0
+    flush_every: int = 0
+    profile: bool = False
+
+    def to_c(self) -> _lib.Config:
+        return _lib.Config(self.particles, self.inverse_filling, self.n_walkers,
+                           self.lanes_per_walker, self.step_sigma, self.guide, self.seed,
+                           self.radius_scale, self.init_radius, self.gram_mode,
+                           self.angular_probe, self.flush_every, 1 if self.profile else 0)
+
+
+class Sampler:
+    """One sampling context on the current CUDA device (wraps lemc_ctx)."""
+
+    def __init__(self, cfg: SamplerConfig, sectors, guide_rows=None):
+        self.lib = _lib.load()
+        self.cfg = cfg
+        self._h = C.c_void_p()
+        c = cfg.to_c()
+        check(self.lib.lemc_create(C.byref(c), C.byref(self._h)), "lemc_create")
+        self.sectors = list(sectors)
+        sec = np.ascontiguousarray(self.sectors, dtype=np.int32)
+        check(self.lib.lemc_set_sectors(self._h, i32ptr(sec), len(sec)), "lemc_set_sectors")
+        if guide_rows is not None:
+            gr = np.ascontiguousarray(guide_rows, dtype=np.int32)
+            check(self.lib.lemc_set_guide_rows(self._h, i32ptr(gr), len(gr)), "lemc_set_guide_rows")
+        self.dims = []
+        for s in range(len(self.sectors)):
+            d = C.c_int()
+            check(self.lib.lemc_sector_dim(self._h, s, C.byref(d)), "lemc_sector_dim")
+            self.dims.append(d.value)
+        d = C.c_int()
+        check(self.lib.lemc_total_dim(self._h, C.byref(d)), "lemc_total_dim")
+        self.total_dim = d.value
+
+    def close(self):
+        if self._h:
+            self.lib.lemc_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def init_walkers(self, xy: np.ndarray | None = None):
+        if xy is None:
+            check(self.lib.lemc_init_walkers(self._h, None), "lemc_init_walkers")
+        else:
+            a = np.ascontiguousarray(xy, dtype=np.float32)
+            check(self.lib.lemc_init_walkers(self._h, fptr(a.ravel())), "lemc_init_walkers")
+
+    def run(self, n_sweeps: int, measure: bool = True):
+        check(self.lib.lemc_run(self._h, int(n_sweeps), 1 if measure else 0), "lemc_run")
+
+    def reset(self):
+        check(self.lib.lemc_reset_accumulators(self._h), "lemc_reset_accumulators")
+
+    def synchronize(self):
+        check(self.lib.lemc_synchronize(self._h), "lemc_synchronize")
+
+    def gram(self, sector_index: int):
+        D = self.dims[sector_index]
+        bufs = [np.zeros(2 * D * D) for _ in range(3)]
+        n = C.c_double()
+        check(self.lib.lemc_read_gram(self._h, sector_index, *[dptr(b) for b in bufs], C.byref(n)),
+              "lemc_read_gram")
+        return tuple(_cplx(b, D) for b in bufs) + (n.value,)
+
+    def cross(self, sa: int, sb: int):
+        Da, Db = self.dims[sa], self.dims[sb]
+        bufs = [np.zeros(2 * Da * Db) for _ in range(3)]
+        check(self.lib.lemc_read_cross(self._h, sa, sb, *[dptr(b) for b in bufs]), "lemc_read_cross")
+        return tuple(b.view(np.complex128).reshape(Da, Db) for b in bufs)
+
+    def rows(self, omega: float, kappa: float):
+        D = self.total_dim
+        fg, gg, fh = np.zeros(2 * D * D), np.zeros(D * D), np.zeros(2 * D * D)
+        n = np.zeros(D)
+        check(self.lib.lemc_read_rows(self._h, omega, kappa, dptr(fg), dptr(gg), dptr(fh), dptr(n)),
+              "lemc_read_rows")
+        return _cplx(fg, D), gg.reshape(D, D), _cplx(fh, D), n
+
+    def stats(self) -> _lib.Stats:
+        st = _lib.Stats()
+        check(self.lib.lemc_read_stats(self._h, C.byref(st)), "lemc_read_stats")
+        return st
+
+    def positions(self) -> np.ndarray:
+        W, N = self.cfg.n_walkers, self.cfg.particles
+        out = np.zeros(W * N * 2, dtype=np.float32)
+        check(self.lib.lemc_read_positions(self._h, fptr(out)), "lemc_read_positions")
+        return out.reshape(W, N, 2)
+
+    def series(self) -> np.ndarray:
+        n = C.c_int()
+        check(self.lib.lemc_read_series(self._h, None, 0, C.byref(n)), "lemc_read_series")
+        out = np.zeros(8 * max(1, n.value))
+        check(self.lib.lemc_read_series(self._h, dptr(out), n.value, C.byref(n)), "lemc_read_series")
+        return out[: 8 * n.value].reshape(n.value, 8)
