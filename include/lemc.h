@@ -74,7 +74,8 @@ typedef struct lemc_config {
   int32_t particles;        /* N                                              */
   int32_t inverse_filling;  /* m (nu = 1/m)                                   */
   int32_t n_walkers;        /* W, independent Markov chains                  */
-  int32_t lanes_per_walker; /* G in {1,2,4,8,16,32}; 0 = autotuned            */
+  int32_t lanes_per_walker; /* G in {1,2,4,8,16,32}; 0 = heuristic, -1 = autotuned at
+                               lemc_init_walkers by timing every feasible G    */
   float step_sigma;         /* Gaussian single-particle step (l_B)           */
   int32_t guide;            /* enum lemc_guide                               */
   uint64_t seed;            /* Philox-4x32-10 key                            */
@@ -83,7 +84,7 @@ typedef struct lemc_config {
   int32_t gram_mode;        /* enum lemc_gram_mode                           */
   int32_t angular_probe;    /* l of the cos/sin weight planes (0 = off)      */
   int32_t flush_every;      /* tcgen05 path: K-chunks per FP64 flush (0=auto) */
-  int32_t reserved0;
+  int32_t profile;          /* 1: time each kernel family with CUDA events   */
 } lemc_config;
 
 /* Statistics of a context after lemc_run(). */
@@ -132,6 +133,8 @@ LEMC_API int lemc_partitions(int particles, const int32_t* sectors, int n_sector
  * partitions on the device and the capacity checks.                         */
 LEMC_API int lemc_create(const lemc_config* cfg, lemc_ctx** out);
 LEMC_API int lemc_destroy(lemc_ctx* ctx);
+/* Walker width G in use (after autotuning). */
+LEMC_API int lemc_lanes_per_walker(const lemc_ctx* ctx, int* lanes);
 /* Select the angular-momentum sectors whose basis is sampled. */
 LEMC_API int lemc_set_sectors(lemc_ctx* ctx, const int32_t* sectors, int n_sectors);
 /* Guide rows for LEMC_GUIDE_ROW: walker w samples |P_{rows[w % n]}|^2 |Psi|^2,
@@ -149,6 +152,9 @@ LEMC_API int lemc_run(lemc_ctx* ctx, int n_sweeps, int measure);
 /* Zero every accumulator (samples, Gram matrices, series, acceptance). */
 LEMC_API int lemc_reset_accumulators(lemc_ctx* ctx);
 LEMC_API int lemc_synchronize(lemc_ctx* ctx);
+/* The context's CUDA stream (cudaStream_t), for callers that order their own
+ * work or device timers after the context's kernels. */
+LEMC_API int lemc_stream(lemc_ctx* ctx, void** stream);
 
 /* Basis dimension of a selected sector and of all selected sectors. */
 LEMC_API int lemc_sector_dim(const lemc_ctx* ctx, int sector_index, int* dim);

@@ -39,7 +39,7 @@ class Config(C.Structure):
                 ("step_sigma", C.c_float), ("guide", C.c_int32), ("seed", C.c_uint64),
                 ("radius_scale", C.c_double), ("init_radius", C.c_double),
                 ("gram_mode", C.c_int32), ("angular_probe", C.c_int32),
-                ("flush_every", C.c_int32), ("reserved0", C.c_int32)]
+                ("flush_every", C.c_int32), ("profile", C.c_int32)]
 
 
 class Stats(C.Structure):
@@ -72,11 +72,13 @@ _SIGNATURES = {
     "lemc_create": ([C.POINTER(Config), C.POINTER(_P)], _I),
     "lemc_destroy": ([_P], _I),
     "lemc_set_sectors": ([_P, _I32P, _I], _I),
+    "lemc_lanes_per_walker": ([_P, _IP], _I),
     "lemc_set_guide_rows": ([_P, _I32P, _I], _I),
     "lemc_init_walkers": ([_P, _FP], _I),
     "lemc_run": ([_P, _I, _I], _I),
     "lemc_reset_accumulators": ([_P], _I),
     "lemc_synchronize": ([_P], _I),
+    "lemc_stream": ([_P, C.POINTER(_P)], _I),
     "lemc_sector_dim": ([_P, _I, _IP], _I),
     "lemc_total_dim": ([_P, _IP], _I),
     "lemc_read_gram": ([_P, _I, _DP, _DP, _DP, _DP], _I),

@@ -138,6 +138,8 @@ struct lemc_ctx {
   DevBuf<int> err;
   // tcgen05 path
   std::vector<TcTile> tc_tiles;
+  int tc_ntiles = 0, tc_npi = 0, tc_npj = 0, tc_maxdim = 0;
+  DevBuf<int> d_tile_of;
   DevBuf<TcTile> d_tc_tiles;
   DevBuf<double> tc_partials;
   int tc_splits = 1;
@@ -148,6 +150,7 @@ struct lemc_ctx {
   std::vector<double> host_series;  // [meas][8]
   double ms_sweep = 0, ms_basis = 0, ms_gram = 0;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  std::vector<cudaEvent_t> pev;  // per-step profiling events (profile mode)
 };
 
 namespace {
@@ -155,7 +158,7 @@ namespace {
 int pick_lanes(int N) {
   // walker width: aim for about 6-12 particles per lane
   int G = 1;
-  while (G < 32 && (N + G - 1) / G > 12) G *= 2;
+  while (G < 32 && (N + G - 1) / G > 16) G *= 2;
   while (G > 1 && !sweep_config_ok(G, N)) G /= 2;
   while (G < 32 && !sweep_config_ok(G, N)) G *= 2;
   return G;
@@ -318,9 +321,9 @@ int gram_step(lemc_ctx* c, const float* V, const float* rec_w, int W, int mode) 
                             c->stream);
   }
   if (c->tc_tiles.empty()) LEMC_TRY(setup_tc(c));
-  int s = launch_gram_tc(V, c->Wpad, rec_w, W, c->Wpad, c->d_tc_tiles.p, int(c->tc_tiles.size()),
-                         c->tc_splits, c->tc_partials.p, mode, c->cfg.flush_every, c->err.p,
-                         c->stream);
+  int s = launch_gram_tc_rows(V, c->Wpad, 2 * c->D, rec_w, W, c->Wpad, c->d_tc_tiles.p,
+                              int(c->tc_tiles.size()), c->tc_splits, c->tc_partials.p, mode,
+                              c->cfg.flush_every, c->err.p, c->stream);
   if (s != LEMC_OK) return s;
   // cross-sector planes (cos/sin/user) are small: FP64 path
   if (c->n_cross_jobs > 0) {
@@ -351,6 +354,16 @@ int setup_tc(lemc_ctx* c) {
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, dev);
   const int nt = int(tiles.size());
+  c->tc_ntiles = nt;
+  c->tc_npi = (rows + 127) / 128;
+  c->tc_npj = (rows + 31) / 32;
+  std::vector<int> tile_of(size_t(c->tc_npi) * c->tc_npj, -1);
+  for (int t = 0; t < nt; ++t) tile_of[(tiles[t].first / 128) * c->tc_npj + tiles[t].second / 32] = t;
+  LEMC_TRY(c->d_tile_of.alloc(tile_of.size()));
+  LEMC_CUDA(cudaMemcpy(c->d_tile_of.p, tile_of.data(), sizeof(int) * tile_of.size(),
+                       cudaMemcpyHostToDevice));
+  c->tc_maxdim = 0;
+  for (int d : c->basis.sector_dim) c->tc_maxdim = std::max(c->tc_maxdim, d);
   c->tc_splits = std::max(1, std::min((sm + nt - 1) / nt, c->Wpad / 256));
   c->tc_tiles.clear();
   for (int s = 0; s < c->tc_splits; ++s)
@@ -359,7 +372,7 @@ int setup_tc(lemc_ctx* c) {
   LEMC_TRY(c->d_tc_tiles.alloc(c->tc_tiles.size()));
   LEMC_CUDA(cudaMemcpy(c->d_tc_tiles.p, c->tc_tiles.data(), sizeof(TcTile) * c->tc_tiles.size(),
                        cudaMemcpyHostToDevice));
-  const size_t slot = size_t(128) * 96;
+  const size_t slot = size_t(kTcSlot);
   LEMC_TRY(c->tc_partials.alloc(slot * c->tc_tiles.size()));
   LEMC_CUDA(cudaMemsetAsync(c->tc_partials.p, 0, sizeof(double) * slot * c->tc_tiles.size(),
                             c->stream));
@@ -380,11 +393,12 @@ int setup_tc(lemc_ctx* c) {
 // partials are zeroed afterwards).
 int flush_tc(lemc_ctx* c) {
   if (c->tc_tiles.empty()) return LEMC_OK;
-  LEMC_TRY(launch_gram_tc_reduce(c->tc_partials.p, c->d_tc_tiles.p, int(c->tc_tiles.size()),
-                                 c->tc_splits, c->d_sec_row.p, c->d_sec_dim.p, c->d_sec_goff.p,
-                                 int(c->sec_row.size()), c->gram.p, c->stream));
-  LEMC_CUDA(cudaMemsetAsync(c->tc_partials.p, 0,
-                            sizeof(double) * 128 * 96 * c->tc_tiles.size(), c->stream));
+  LEMC_TRY(launch_gram_tc_reduce(c->tc_partials.p, c->d_tile_of.p, c->tc_npi, c->tc_npj,
+                                 c->tc_ntiles, c->tc_splits, c->d_sec_row.p, c->d_sec_dim.p,
+                                 c->d_sec_goff.p, int(c->sec_row.size()), c->tc_maxdim, c->gram.p,
+                                 c->gram_plane, c->stream));
+  LEMC_CUDA(cudaMemsetAsync(c->tc_partials.p, 0, sizeof(double) * kTcSlot * c->tc_tiles.size(),
+                            c->stream));
   return LEMC_OK;
 }
 
@@ -471,7 +485,7 @@ int lemc_create(const lemc_config* cfg, lemc_ctx** out) {
   c->Wpad = (c->W + 63) / 64 * 64;
   const double rcl = std::sqrt(2.0 * c->m * c->N);
   c->R = float(cfg->radius_scale > 0 ? cfg->radius_scale : rcl);
-  c->profile = cfg->reserved0 != 0;
+  c->profile = cfg->profile != 0;
   c->G = cfg->lanes_per_walker > 0 ? cfg->lanes_per_walker : pick_lanes(c->N);
   if (!sweep_config_ok(c->G, c->N)) {
     delete c;
@@ -516,12 +530,14 @@ int lemc_destroy(lemc_ctx* c) {
   c->rowacc.release();
   c->err.release();
   c->d_tc_tiles.release();
+  c->d_tile_of.release();
   c->tc_partials.release();
   c->d_sec_row.release();
   c->d_sec_dim.release();
   c->d_sec_goff.release();
   for (auto& e : c->ev)
     if (e) cudaEventDestroy(e);
+  for (auto& e : c->pev) cudaEventDestroy(e);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return LEMC_OK;
@@ -616,6 +632,47 @@ int lemc_set_guide_rows(lemc_ctx* c, const int32_t* rows, int n_rows) {
   return upload_guide(c);
 }
 
+// Walker-width autotuner: times a few sweeps per feasible G on a copy of the
+// current walkers (restored afterwards, sweep counter unchanged) and keeps
+// the fastest.  Used when lanes_per_walker < 0.
+static int autotune_lanes(lemc_ctx* c) {
+  DevBuf<float2> save;
+  LEMC_TRY(save.alloc(size_t(c->W) * c->N));
+  LEMC_CUDA(cudaMemcpyAsync(save.p, c->pos.p, sizeof(float2) * c->W * c->N,
+                            cudaMemcpyDeviceToDevice, c->stream));
+  const int keep_G = c->G;
+  float best = 1e30f;
+  int bestG = keep_G;
+  for (int G = 1; G <= 32; G *= 2) {
+    if (!sweep_config_ok(G, c->N)) continue;
+    c->G = G;
+    LEMC_TRY(sweep_once(c, 1, 0));  // warm the instruction cache / attributes
+    LEMC_CUDA(cudaEventRecord(c->ev[0], c->stream));
+    LEMC_TRY(sweep_once(c, 3, 0));
+    LEMC_CUDA(cudaEventRecord(c->ev[1], c->stream));
+    LEMC_CUDA(cudaEventSynchronize(c->ev[1]));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
+    if (ms < best) {
+      best = ms;
+      bestG = G;
+    }
+    LEMC_CUDA(cudaMemcpyAsync(c->pos.p, save.p, sizeof(float2) * c->W * c->N,
+                              cudaMemcpyDeviceToDevice, c->stream));
+  }
+  c->G = bestG;
+  if (c->accepted.p) LEMC_CUDA(cudaMemsetAsync(c->accepted.p, 0, 4 * c->W, c->stream));
+  LEMC_CUDA(cudaStreamSynchronize(c->stream));
+  save.release();
+  return LEMC_OK;
+}
+
+int lemc_lanes_per_walker(const lemc_ctx* c, int* G) {
+  if (!c || !G) return LEMC_ERR_ARG;
+  *G = c->G;
+  return LEMC_OK;
+}
+
 int lemc_init_walkers(lemc_ctx* c, const float* host_xy) {
   if (!c) return LEMC_ERR_ARG;
   if (host_xy) {
@@ -627,6 +684,7 @@ int lemc_init_walkers(lemc_ctx* c, const float* host_xy) {
                                  uint32_t(c->cfg.seed >> 32), c->stream));
   }
   c->walkers_ready = true;
+  if (c->cfg.lanes_per_walker < 0) LEMC_TRY(autotune_lanes(c));
   return LEMC_OK;
 }
 
@@ -654,6 +712,12 @@ int lemc_synchronize(lemc_ctx* c) {
   return LEMC_OK;
 }
 
+int lemc_stream(lemc_ctx* c, void** stream) {
+  if (!c || !stream) return LEMC_ERR_ARG;
+  *stream = static_cast<void*>(c->stream);
+  return LEMC_OK;
+}
+
 int lemc_run(lemc_ctx* c, int n_sweeps, int measure) {
   if (!c || n_sweeps < 0) return LEMC_ERR_ARG;
   if (!c->walkers_ready) return LEMC_ERR_STATE;
@@ -671,36 +735,41 @@ int lemc_run(lemc_ctx* c, int n_sweeps, int measure) {
   }
   LEMC_TRY(c->series.alloc(size_t(8) * n_sweeps));
   LEMC_CUDA(cudaMemsetAsync(c->series.p, 0, sizeof(double) * 8 * n_sweeps, c->stream));
-  float tms[3] = {0, 0, 0};
+  // profile mode: four events per step, read after the loop (no per-step sync)
+  if (c->profile) {
+    while (c->pev.size() < size_t(4) * n_sweeps) {
+      cudaEvent_t e;
+      LEMC_CUDA(cudaEventCreate(&e));
+      c->pev.push_back(e);
+    }
+  }
   for (int s = 0; s < n_sweeps; ++s) {
-    if (c->profile) cudaEventRecord(c->ev[0], c->stream);
+    if (c->profile) LEMC_CUDA(cudaEventRecord(c->pev[4 * s], c->stream));
     LEMC_TRY(sweep_once(c, 1, 1));
     c->sweeps += 1;
-    if (c->profile) cudaEventRecord(c->ev[1], c->stream);
+    if (c->profile) LEMC_CUDA(cudaEventRecord(c->pev[4 * s + 1], c->stream));
     LEMC_TRY(launch_basis(c->rec_p.p, c->W, c->K, c->N, c->prog.p, c->n_nodes, c->V.p, c->Wpad,
                           c->series.p + 8 * size_t(s), c->stream));
-    if (c->profile) cudaEventRecord(c->ev[2], c->stream);
+    if (c->profile) LEMC_CUDA(cudaEventRecord(c->pev[4 * s + 2], c->stream));
     LEMC_TRY(gram_step(c, c->V.p, c->rec_w.p, c->W, c->cfg.gram_mode));
-    if (c->profile) {
-      cudaEventRecord(c->ev[3], c->stream);
-      LEMC_CUDA(cudaEventSynchronize(c->ev[3]));
-      float t;
-      cudaEventElapsedTime(&t, c->ev[0], c->ev[1]);
-      tms[0] += t;
-      cudaEventElapsedTime(&t, c->ev[1], c->ev[2]);
-      tms[1] += t;
-      cudaEventElapsedTime(&t, c->ev[2], c->ev[3]);
-      tms[2] += t;
-    }
+    if (c->profile) LEMC_CUDA(cudaEventRecord(c->pev[4 * s + 3], c->stream));
     c->meas += 1;
   }
-  c->ms_sweep += tms[0];
-  c->ms_basis += tms[1];
-  c->ms_gram += tms[2];
   std::vector<double> ser(size_t(8) * n_sweeps);
   LEMC_CUDA(cudaMemcpyAsync(ser.data(), c->series.p, sizeof(double) * ser.size(),
                             cudaMemcpyDeviceToHost, c->stream));
   LEMC_TRY(lemc_synchronize(c));
+  if (c->profile) {
+    for (int s = 0; s < n_sweeps; ++s) {
+      float t = 0;
+      cudaEventElapsedTime(&t, c->pev[4 * s], c->pev[4 * s + 1]);
+      c->ms_sweep += t;
+      cudaEventElapsedTime(&t, c->pev[4 * s + 1], c->pev[4 * s + 2]);
+      c->ms_basis += t;
+      cudaEventElapsedTime(&t, c->pev[4 * s + 2], c->pev[4 * s + 3]);
+      c->ms_gram += t;
+    }
+  }
   for (double& v : ser) v /= c->W;
   c->host_series.insert(c->host_series.end(), ser.begin(), ser.end());
   return LEMC_OK;
@@ -725,7 +794,7 @@ int lemc_read_gram(lemc_ctx* c, int s, double* S, double* H2, double* H4, double
   if (!c) return LEMC_ERR_ARG;
   if (!c->has_basis) return LEMC_ERR_STATE;
   if (s < 0 || s >= int(c->sec_row.size())) return LEMC_ERR_ARG;
-  if (c->cfg.gram_mode != LEMC_GRAM_FP64) LEMC_TRY(flush_tc(c));
+  LEMC_TRY(flush_tc(c));
   const int dim = c->basis.sector_dim[s];
   const size_t off = 2 * size_t(c->sec_goff[s]);
   const size_t bytes = sizeof(double) * 2 * dim * dim;
@@ -855,11 +924,22 @@ int lemc_sweep_device(void* pos, int W, int N, int m, float sigma, uint64_t seed
   return launch_sweep(a, G, static_cast<cudaStream_t>(stream));
 }
 
+// Work launched on a caller's stream is ordered before everything the context
+// issues afterwards on its own (non-blocking) stream.
+static int order_after(lemc_ctx* c, cudaStream_t user) {
+  if (user == c->stream) return LEMC_OK;
+  LEMC_CUDA(cudaEventRecord(c->ev[3], user));
+  LEMC_CUDA(cudaStreamWaitEvent(c->stream, c->ev[3], 0));
+  return LEMC_OK;
+}
+
 int lemc_basis_device(lemc_ctx* c, const void* rec_p, int W, void* V, int ldv, void* stream) {
   if (!c || !rec_p || !V || W <= 0 || ldv < W) return LEMC_ERR_ARG;
   if (!c->has_basis) return LEMC_ERR_STATE;
-  return launch_basis(static_cast<const float2*>(rec_p), W, c->K, c->N, c->prog.p, c->n_nodes,
-                      static_cast<float*>(V), ldv, nullptr, static_cast<cudaStream_t>(stream));
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  LEMC_TRY(launch_basis(static_cast<const float2*>(rec_p), W, c->K, c->N, c->prog.p, c->n_nodes,
+                        static_cast<float*>(V), ldv, nullptr, st));
+  return order_after(c, st);
 }
 
 int lemc_gram_device(lemc_ctx* c, const void* V, const void* rec_w, int W, int ldv, int mode,
@@ -867,11 +947,15 @@ int lemc_gram_device(lemc_ctx* c, const void* V, const void* rec_w, int W, int l
   if (!c || !V || !rec_w || W <= 0) return LEMC_ERR_ARG;
   if (!c->has_basis) return LEMC_ERR_STATE;
   if (ldv != c->Wpad || W != c->W) return LEMC_ERR_ARG;
-  cudaStream_t saved = c->stream;
-  if (stream) c->stream = static_cast<cudaStream_t>(stream);
-  const int s = gram_step(c, static_cast<const float*>(V), static_cast<const float*>(rec_w), W, mode);
-  c->stream = saved;
-  return s;
+  // the context's accumulators are only touched on its own stream: wait for the
+  // caller's stream, run there, and hand the ordering back
+  cudaStream_t user = static_cast<cudaStream_t>(stream);
+  LEMC_CUDA(cudaEventRecord(c->ev[2], user));
+  LEMC_CUDA(cudaStreamWaitEvent(c->stream, c->ev[2], 0));
+  LEMC_TRY(gram_step(c, static_cast<const float*>(V), static_cast<const float*>(rec_w), W, mode));
+  LEMC_CUDA(cudaEventRecord(c->ev[3], c->stream));
+  LEMC_CUDA(cudaStreamWaitEvent(user, c->ev[3], 0));
+  return LEMC_OK;
 }
 
 }  // extern "C"

@@ -21,7 +21,7 @@ struct SweepArgs {
   const int32_t* guide_pairs;  // [rows][2*kMaxGuideParts] (part, mult)
   const int32_t* guide_npairs; // [rows]
   int* err;                 // device error word (may be null)
-  int W, N, Npad, m, K;
+  int W, N, Npad, T2, m, K;  // Npad >= T2 * G, set by sweep_layout()
   float sigma, invR;
   uint32_t seed_lo, seed_hi;
   uint32_t sweep0;
@@ -53,6 +53,10 @@ struct GramJob {
 
 int launch_sweep(const SweepArgs& a, int lanes_per_walker, cudaStream_t st);
 size_t sweep_smem_bytes(int lanes_per_walker, int Npad);
+// Shared-memory layout of a walker: T2 slots per lane (ceil(N/G) rounded up
+// to even) and a per-walker stride Npad >= T2*G chosen so that the walker
+// groups of a half-warp hit disjoint bank pairs (Npad = G mod 16 for G < 16).
+void sweep_layout(int lanes_per_walker, int N, int* T2, int* Npad);
 bool sweep_config_ok(int lanes_per_walker, int N);
 
 int launch_init_walkers(float2* pos, int W, int N, float radius, uint32_t seed_lo,
@@ -75,14 +79,16 @@ struct TcTile {
   int row0;   // first V row of the 128-row A panel
   int col0;   // first V row of the 32-row B panel
   int ksplit; // walker split index
-  int slot;   // FP64 partial slot index
+  int slot;   // FP64 partial slot index (ksplit * n_tiles + tile)
 };
-int launch_gram_tc(const float* V, int ldv, const float* rec_w, int W, int Wpad,
-                   const TcTile* tiles, int n_tiles, int n_splits, double* partials,
-                   int mode, int flush_every, int* err, cudaStream_t st);
-int launch_gram_tc_reduce(const double* partials, const TcTile* tiles, int n_tiles,
-                          int n_splits, const int32_t* sec_row, const int32_t* sec_dim,
-                          const int32_t* sec_goff, int n_sec, double* gram,
-                          cudaStream_t st);
+int launch_gram_tc_rows(const float* V, int ldv, int total_rows, const float* rec_w, int W,
+                        int Wpad, const TcTile* tiles, int n_jobs, int n_splits, double* partials,
+                        int mode, int flush_every, int* err, cudaStream_t st);
+int launch_gram_tc_reduce(const double* partials, const int* tile_of, int n_pi, int n_pj,
+                          int n_tiles, int n_splits, const int32_t* sec_row,
+                          const int32_t* sec_dim, const int32_t* sec_goff, int n_sec,
+                          int max_dim, double* gram, size_t plane, cudaStream_t st);
+size_t gram_tc_smem_bytes();
+constexpr int kTcSlot = 128 * 96;  // doubles per partial slot
 
 }  // namespace lemc

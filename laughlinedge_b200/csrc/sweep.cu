@@ -10,8 +10,9 @@
 // is one walker per warp).  The walker's coordinates live in shared memory;
 // lane l of the group owns particles j = l, l+G, l+2G, ...  For a move of
 // particle i every lane accumulates the products prod |z'-z_j|^2 and
-// prod |z-z_j|^2 over its particles (one log2 per 8 pairs keeps FP32 in
-// range), the G partial log-ratios are combined with a butterfly of
+// prod |z-z_j|^2 over its particles in two independent chains (one log2 per
+// chain every 16 slots keeps FP32 in range), the G partial log-ratios are
+// combined with a butterfly of
 // __shfl_xor_sync (all lanes end with bitwise identical sums, hence identical
 // accept decisions), and the owner lane commits the move.
 //
@@ -79,10 +80,11 @@ sweep_kernel(const SweepArgs a) {
   const int w = blockIdx.x * WPB + wl;
   const bool live = w < a.W;
   const int N = a.N;
+  const int T2 = a.T2;  // particle slots per lane, rounded up to even
   float2* zs = sm_pos + (size_t)wl * a.Npad;
 
-  for (int j = gl; j < N; j += G)
-    zs[j] = live ? a.pos[(size_t)w * N + j] : make_float2(3.f * j + 1.f, 0.25f * j);
+  for (int j = gl; j < T2 * G; j += G)
+    zs[j] = (live && j < N) ? a.pos[(size_t)w * N + j] : make_float2(3.f * j + 1.f, 0.25f * j);
   __syncwarp();
 
   // ---- guide state: the distinct parts of the walker's guide partition ----
@@ -154,26 +156,29 @@ sweep_kernel(const SweepArgs a) {
         const float yn = __shfl_sync(0xffffffffu, pzy, b, G);
         const float lu = __shfl_sync(0xffffffffu, plu, b, G);
 
-        // Jastrow log2-ratio over this lane's particles
+        // Jastrow log2-ratio over this lane's particles: two independent
+        // product chains, masked (not branched) for j == i and the padding,
+        // one log2 per chain every 16 slots keeps FP32 in range.
         float part = 0.f;
-        float num = 1.f, den = 1.f;
-        int cnt = 0;
-        for (int j = gl; j < N; j += G) {
-          if (j != im) {
-            const float2 zj = zs[j];
-            const float dx = xn - zj.x, dy = yn - zj.y;
-            const float ex = zo.x - zj.x, ey = zo.y - zj.y;
-            num *= fmaf(dx, dx, dy * dy);
-            den *= fmaf(ex, ex, ey * ey);
-            if (++cnt == 8) {
-              part += __log2f(num) - __log2f(den);
-              num = 1.f;
-              den = 1.f;
-              cnt = 0;
-            }
+        for (int c0 = 0; c0 < T2; c0 += 16) {
+          float n0 = 1.f, d0 = 1.f, n1 = 1.f, d1 = 1.f;
+          const int cend = min(T2, c0 + 16);
+          for (int t = c0; t < cend; t += 2) {
+            const int ja = gl + t * G, jb = ja + G;
+            const float2 za = zs[ja], zb = zs[jb];
+            const float ax = xn - za.x, ay = yn - za.y, ex = zo.x - za.x, ey = zo.y - za.y;
+            const float bx = xn - zb.x, by = yn - zb.y, fx = zo.x - zb.x, fy = zo.y - zb.y;
+            const float pa = fmaf(ax, ax, ay * ay), qa = fmaf(ex, ex, ey * ey);
+            const float pb = fmaf(bx, bx, by * by), qb = fmaf(fx, fx, fy * fy);
+            const bool va = (ja < N) && (ja != im);
+            const bool vb = (jb < N) && (jb != im);
+            n0 *= va ? pa : 1.f;
+            d0 *= va ? qa : 1.f;
+            n1 *= vb ? pb : 1.f;
+            d1 *= vb ? qb : 1.f;
           }
+          part += (__log2f(n0) + __log2f(n1)) - (__log2f(d0) + __log2f(d1));
         }
-        part += __log2f(num) - __log2f(den);
         part *= mf;
 
         // guide polynomial ratio |P_a(z')/P_a(z)|^2 (row guide)
@@ -303,17 +308,30 @@ int launch_g(const SweepArgs& a, cudaStream_t st) {
 
 }  // namespace
 
+void sweep_layout(int G, int N, int* T2, int* Npad) {
+  int t = (N + G - 1) / G;
+  t += (t & 1);
+  int np = t * G;
+  if (G < 16) np += ((G - np) % 16 + 16) % 16;
+  *T2 = t;
+  *Npad = np;
+}
+
 size_t sweep_smem_bytes(int G, int Npad) {
   return size_t((kSweepThreads / 32) * (32 / G)) * Npad * sizeof(float2);
 }
 
 bool sweep_config_ok(int G, int N) {
   if (G != 1 && G != 2 && G != 4 && G != 8 && G != 16 && G != 32) return false;
-  return sweep_smem_bytes(G, N) <= 227 * 1024;
+  int t2, np;
+  sweep_layout(G, N, &t2, &np);
+  return sweep_smem_bytes(G, np) <= 227 * 1024;
 }
 
-int launch_sweep(const SweepArgs& a, int G, cudaStream_t st) {
-  if (a.K > kMaxDegree || a.N <= 1 || a.W <= 0) return LEMC_ERR_ARG;
+int launch_sweep(const SweepArgs& a_in, int G, cudaStream_t st) {
+  if (a_in.K > kMaxDegree || a_in.N <= 1 || a_in.W <= 0) return LEMC_ERR_ARG;
+  SweepArgs a = a_in;
+  sweep_layout(G, a.N, &a.T2, &a.Npad);
   switch (G) {
     case 1: return launch_g<1>(a, st);
     case 2: return launch_g<2>(a, st);

@@ -160,6 +160,16 @@ class Sampler:
     def reset(self):
         check(self.lib.lemc_reset_accumulators(self._h), "lemc_reset_accumulators")
 
+    def lanes_per_walker(self) -> int:
+        g = C.c_int()
+        check(self.lib.lemc_lanes_per_walker(self._h, C.byref(g)), "lemc_lanes_per_walker")
+        return g.value
+
+    def stream(self) -> int:
+        h = C.c_void_p()
+        check(self.lib.lemc_stream(self._h, C.byref(h)), "lemc_stream")
+        return h.value or 0
+
     def synchronize(self):
         check(self.lib.lemc_synchronize(self._h), "lemc_synchronize")
 

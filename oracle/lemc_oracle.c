@@ -296,7 +296,7 @@ static cx basis_value(const cx* p, int N, const int* pairs, int np) {
 static void run_common(int mode, int N, int m, int W, double sigma, uint64_t seed, int n_burn,
                        int n_meas, double invR, double init_radius, int D, const int* rows_np,
                        const int* pairs, const int* rows_dL, int K, double* o1, double* o2,
-                       double* o3, double* o4, double* n_row, int nthreads) {
+                       double* o3, double* o4, double* n_row, double* series, int nthreads) {
   const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
   const size_t DD = (size_t)D * D;
   memset(o1, 0, sizeof(double) * 2 * DD);
@@ -314,6 +314,7 @@ static void run_common(int mode, int N, int m, int W, double sigma, uint64_t see
       1;
 #endif
   double* priv = (double*)calloc((size_t)nth * 7 * DD + 1, sizeof(double));
+  double* pser = series ? (double*)calloc((size_t)nth * n_meas * 8 + 1, sizeof(double)) : NULL;
   float* pos = (float*)malloc(sizeof(float) * 2 * (size_t)W * N);
   orc_init(pos, W, N, init_radius, seed);
 #ifdef _OPENMP
@@ -341,6 +342,8 @@ static void run_common(int mode, int N, int m, int W, double sigma, uint64_t see
     for (int s = 0; s < n_meas; ++s) {
       walker_sweeps(z, N, m, sigma, k0, k1, (uint32_t)w, (uint32_t)(n_burn + s), 1, invR, gk, gr, np);
       orc_measure(z, 1, N, K, invR, 0, rp, rw);
+      if (pser)
+        for (int q = 0; q < 8 && q < 2 * K; ++q) pser[((size_t)tid * n_meas + s) * 8 + q] += rp[q];
       for (int b = 0; b < D; ++b) v[b] = basis_value((const cx*)rp, N, pairs + b * 2 * ORC_MAXK, rows_np[b]);
       if (mode == 0) {
         const cx va = v[row];
@@ -382,6 +385,15 @@ static void run_common(int mode, int N, int m, int W, double sigma, uint64_t see
       for (size_t o = 0; o < 2 * DD; ++o) { o1[o] += acc[o]; o2[o] += acc[2 * DD + o]; o3[o] += acc[4 * DD + o]; }
     }
   }
+  if (pser) {
+    for (int s = 0; s < n_meas; ++s)
+      for (int q = 0; q < 8; ++q) {
+        double v = 0.0;
+        for (int t = 0; t < nth; ++t) v += pser[((size_t)t * n_meas + s) * 8 + q];
+        series[(size_t)s * 8 + q] = v / W;
+      }
+    free(pser);
+  }
   free(priv);
   free(pos);
   (void)o4;
@@ -390,17 +402,18 @@ static void run_common(int mode, int N, int m, int W, double sigma, uint64_t see
 void orc_run_rows(int N, int m, int W, double sigma, uint64_t seed, int n_burn, int n_meas,
                   double invR, double init_radius, int D, const int* rows_np, const int* pairs,
                   const int* rows_dL, int K, double* fg, double* gg, double* fh2, double* fh4,
-                  double* n_row, int nthreads) {
+                  double* n_row, double* series, int nthreads) {
   run_common(0, N, m, W, sigma, seed, n_burn, n_meas, invR, init_radius, D, rows_np, pairs, rows_dL,
-             K, fg, gg, fh2, fh4, n_row, nthreads);
+             K, fg, gg, fh2, fh4, n_row, series, nthreads);
 }
 
 void orc_run_gram(int N, int m, int W, double sigma, uint64_t seed, int n_burn, int n_meas,
                   double invR, double init_radius, int D, const int* rows_np, const int* pairs,
-                  const int* rows_dL, int K, double* S, double* H2, double* H4, int nthreads) {
+                  const int* rows_dL, int K, double* S, double* H2, double* H4, double* series,
+                  int nthreads) {
   double dummy[2];
   run_common(1, N, m, W, sigma, seed, n_burn, n_meas, invR, init_radius, D, rows_np, pairs, rows_dL,
-             K, S, H2, H4, dummy, NULL, nthreads);
+             K, S, H2, H4, dummy, NULL, series, nthreads);
 }
 
 int orc_max_threads(void) {

@@ -137,7 +137,8 @@ def _rows_arrays(rows):
 
 def run_rows(N, m, W, sigma, seed, n_burn, n_meas, sectors, R=None, init_radius=None,
              nthreads=0):
-    """Reference estimator (row guides).  Returns dict of raw sums."""
+    """Reference estimator (row guides).  Returns dict of raw sums and the
+    walker-mean series of Re/Im p_1..p_4 per measurement."""
     lib = load()
     rows = partitions(N, sectors)
     D = len(rows)
@@ -150,13 +151,14 @@ def run_rows(N, m, W, sigma, seed, n_burn, n_meas, sectors, R=None, init_radius=
     fh2 = np.zeros(2 * D * D)
     fh4 = np.zeros(2 * D * D)
     nrow = np.zeros(D)
+    series = np.zeros(max(1, n_meas) * 8)
     lib.orc_run_rows(C.c_int(N), C.c_int(m), C.c_int(W), C.c_double(sigma), C.c_uint64(seed),
                      C.c_int(n_burn), C.c_int(n_meas), C.c_double(1.0 / R), C.c_double(init_radius),
                      C.c_int(D), _p(np_), _p(pairs), _p(dl), C.c_int(K), _p(fg), _p(gg), _p(fh2),
-                     _p(fh4), _p(nrow), C.c_int(nthreads))
+                     _p(fh4), _p(nrow), _p(series), C.c_int(nthreads))
     cz = lambda b: b.view(np.complex128).reshape(D, D)
     return {"rows": rows, "fg": cz(fg), "gg": gg.reshape(D, D), "fh2": cz(fh2), "fh4": cz(fh4),
-            "n_row": nrow}
+            "n_row": nrow, "series": series[: 8 * n_meas].reshape(n_meas, 8)}
 
 
 def run_gram(N, m, W, sigma, seed, n_burn, n_meas, sectors, R=None, init_radius=None, nthreads=0):
@@ -171,12 +173,33 @@ def run_gram(N, m, W, sigma, seed, n_burn, n_meas, sectors, R=None, init_radius=
     S = np.zeros(2 * D * D)
     H2 = np.zeros(2 * D * D)
     H4 = np.zeros(2 * D * D)
+    series = np.zeros(max(1, n_meas) * 8)
     lib.orc_run_gram(C.c_int(N), C.c_int(m), C.c_int(W), C.c_double(sigma), C.c_uint64(seed),
                      C.c_int(n_burn), C.c_int(n_meas), C.c_double(1.0 / R), C.c_double(init_radius),
                      C.c_int(D), _p(np_), _p(pairs), _p(dl), C.c_int(K), _p(S), _p(H2), _p(H4),
-                     C.c_int(nthreads))
+                     _p(series), C.c_int(nthreads))
     cz = lambda b: b.view(np.complex128).reshape(D, D)
     return rows, cz(S), cz(H2), cz(H4)
+
+
+def tau_int(series, c=5.0):
+    """Sokal automatic-window integrated autocorrelation time of each column."""
+    x = np.asarray(series, float)
+    out = []
+    for col in x.T:
+        T = len(col)
+        y = col - col.mean()
+        c0 = np.dot(y, y) / T
+        if T < 8 or c0 <= 0:
+            out.append(float("nan"))
+            continue
+        tau = 0.5
+        for t in range(1, T // 2):
+            tau += np.dot(y[:-t], y[t:]) / T / c0
+            if t >= c * tau:
+                break
+        out.append(tau)
+    return np.array(out)
 
 
 def reference_matrices(fg, gg, fh):

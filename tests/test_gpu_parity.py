@@ -155,7 +155,7 @@ def test_gpu_harmonic_degeneracy(lemc, cuda_ctx):
     N, m = 8, 3
     sectors = [1, 2, 3, 4, 5, 6]
     evs, st = _spectra(lemc, N, m, 4096, sectors, 5, 300, 600, 1.0, 0.0)
-    assert 0.3 < st.acceptance < 0.8
+    assert 0.3 < st.acceptance < 0.95
     for dL, ev in zip(sectors, evs):
         lvl = harmonic_level(N, m, dL)
         assert abs(np.mean(ev) - lvl) < 0.005 * lvl, (dL, ev, lvl)

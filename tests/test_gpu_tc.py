@@ -1,0 +1,76 @@
+"""tcgen05 split-precision S/H contraction against the FP64 accumulation of the
+same samples (same V planes, same weights), through the C-ABI."""
+import ctypes as C
+import math
+
+import numpy as np
+import pytest
+
+from test_gpu_parity import dev_sweep
+
+pytestmark = pytest.mark.gpu
+
+# relative error of normalised entries |X_tc - X_fp64| / sqrt(S_aa S_bb), stated per mode
+TOL = {1: 2e-5, 2: 2e-6, 3: 2e-6}
+
+
+def _records(lemc, oracle, torch, N, m, W, sectors, seed, sweeps):
+    R = math.sqrt(2 * m * N)
+    K = max(4, max(sectors))
+    pos0 = oracle.init_walkers(W, N, R, seed)
+    # thermalise a little on the device, then take one measured sweep
+    gpos, _, _, _ = dev_sweep(lemc, torch, pos0, m, 0.3, seed, 0, sweeps, K, R, 0)
+    gpos, rp, rw, _ = dev_sweep(lemc, torch, gpos, m, 0.3, seed, sweeps, 1, K, R, 0, measure=1)
+    return rp, rw
+
+
+def _gram_both(lemc, torch, N, m, W, sectors, rp, rw, mode, flush=0):
+    lib = lemc.load()
+    out = {}
+    Wpad = (W + 63) // 64 * 64
+    for md in (lemc._lib.GRAM_FP64, mode):
+        smp = lemc.Sampler(lemc.SamplerConfig(N, m, W, flush_every=flush), sectors)
+        rec_p = torch.from_numpy(np.ascontiguousarray(rp)).cuda()
+        rec_w = torch.from_numpy(np.ascontiguousarray(rw)).cuda()
+        V = torch.zeros((2 * smp.total_dim, Wpad), dtype=torch.float32, device="cuda")
+        assert lib.lemc_basis_device(smp._h, C.c_void_p(rec_p.data_ptr()), W,
+                                     C.c_void_p(V.data_ptr()), Wpad, None) == 0
+        assert lib.lemc_gram_device(smp._h, C.c_void_p(V.data_ptr()), C.c_void_p(rec_w.data_ptr()),
+                                    W, Wpad, md, None) == 0
+        torch.cuda.synchronize()
+        smp.synchronize()
+        out[md] = [smp.gram(s)[:3] for s in range(len(sectors))]
+        smp.close()
+    return out[lemc._lib.GRAM_FP64], out[mode]
+
+
+def _rel_err(ref, got):
+    worst = 0.0
+    for (S, H2, H4), (S2, H22, H42) in zip(ref, got):
+        d = np.sqrt(np.real(np.diag(S)))
+        nrm = np.outer(d, d)
+        for X, Y, sc in ((S, S2, 1.0), (H2, H22, np.max(np.abs(H2 / nrm))), (H4, H42, np.max(np.abs(H4 / nrm)))):
+            worst = max(worst, float(np.max(np.abs(X - Y) / nrm) / sc))
+    return worst
+
+
+@pytest.mark.parametrize("mode", [1, 2, 3])
+def test_tc_gram_small(lemc, oracle, cuda_ctx, mode):
+    N, m, W = 8, 3, 4096
+    sectors = [0, 1, 2, 3, 4, 5, 6]
+    rp, rw = _records(lemc, oracle, cuda_ctx, N, m, W, sectors, 21, 20)
+    ref, got = _gram_both(lemc, cuda_ctx, N, m, W, sectors, rp, rw, mode)
+    err = _rel_err(ref, got)
+    print(f"mode {mode}: max normalised error {err:.3e}")
+    assert err < TOL[mode]
+
+
+@pytest.mark.parametrize("mode", [1, 2, 3])
+def test_tc_gram_config2_shapes(lemc, oracle, cuda_ctx, mode):
+    N, m, W = 50, 3, 8192
+    sectors = list(range(13))
+    rp, rw = _records(lemc, oracle, cuda_ctx, N, m, W, sectors, 5, 10)
+    ref, got = _gram_both(lemc, cuda_ctx, N, m, W, sectors, rp, rw, mode)
+    err = _rel_err(ref, got)
+    print(f"mode {mode}: max normalised error {err:.3e}")
+    assert err < TOL[mode]
