@@ -138,12 +138,11 @@ struct lemc_ctx {
   DevBuf<int> err;
   // tcgen05 path
   std::vector<TcTile> tc_tiles;
-  int tc_ntiles = 0, tc_npi = 0, tc_npj = 0, tc_maxdim = 0;
-  DevBuf<int> d_tile_of;
+  int tc_ntiles = 0, tc_maxdim = 0;
+  DevBuf<TcSector> d_tc_secs;
   DevBuf<TcTile> d_tc_tiles;
   DevBuf<double> tc_partials;
   int tc_splits = 1;
-  DevBuf<int32_t> d_sec_row, d_sec_dim, d_sec_goff;
 
   bool walkers_ready = false;
   uint64_t sweeps = 0, meas = 0, sweeps_at_reset = 0;
@@ -292,6 +291,7 @@ int sweep_once(lemc_ctx* c, int n_sweeps, int measure) {
   a.guide_npairs = c->d_guide_npairs.p;
   a.err = c->err.p;
   a.W = c->W;
+  a.ldw = c->Wpad;
   a.N = c->N;
   a.Npad = c->N;
   a.m = c->m;
@@ -308,46 +308,62 @@ int sweep_once(lemc_ctx* c, int n_sweeps, int measure) {
   return launch_sweep(a, c->G, c->stream);
 }
 
-int gram_step(lemc_ctx* c, const float* V, const float* rec_w, int W, int mode) {
+int gram_step(lemc_ctx* c, const float* V, const float* rec_w, int ldw, int W, int mode) {
   if (c->cfg.guide == LEMC_GUIDE_ROW) {
-    return launch_row_accumulate(V, c->Wpad, rec_w, W, c->d_row_first.p,
+    return launch_row_accumulate(V, c->Wpad, rec_w, ldw, W, c->d_row_first.p,
                                  int(c->basis.rows.size()), c->D, c->d_row_re.p, c->d_row_im.p,
                                  c->rowacc.p, c->stream);
   }
   if (mode == LEMC_GRAM_FP64) {
     const int splits = std::max(1, std::min(64, W / 1024));
-    return launch_gram_simt(V, c->Wpad, rec_w, W, c->jobs.p, c->n_gram_jobs + c->n_cross_jobs,
+    return launch_gram_simt(V, c->Wpad, rec_w, ldw, W, c->jobs.p, c->n_gram_jobs + c->n_cross_jobs,
                             splits, c->gram.p, c->gram_plane, c->cross.p, c->cross_plane,
                             c->stream);
   }
   if (c->tc_tiles.empty()) LEMC_TRY(setup_tc(c));
-  int s = launch_gram_tc_rows(V, c->Wpad, 2 * c->D, rec_w, W, c->Wpad, c->d_tc_tiles.p,
+  int s = launch_gram_tc_rows(V, c->Wpad, 2 * c->D, rec_w, ldw, c->Wpad, c->d_tc_tiles.p,
                               int(c->tc_tiles.size()), c->tc_splits, c->tc_partials.p, mode,
                               c->cfg.flush_every, c->err.p, c->stream);
   if (s != LEMC_OK) return s;
   // cross-sector planes (cos/sin/user) are small: FP64 path
   if (c->n_cross_jobs > 0) {
     const int splits = std::max(1, std::min(64, W / 1024));
-    s = launch_gram_simt(V, c->Wpad, rec_w, W, c->jobs.p + c->n_gram_jobs, c->n_cross_jobs,
+    s = launch_gram_simt(V, c->Wpad, rec_w, ldw, W, c->jobs.p + c->n_gram_jobs, c->n_cross_jobs,
                          splits, c->gram.p, c->gram_plane, c->cross.p, c->cross_plane, c->stream);
   }
   return s;
 }
 
 int setup_tc(lemc_ctx* c) {
-  // 128-row A panels x 32-row B panels over the block-diagonal support of the
-  // per-sector Gram blocks; each tile covers every column it touches.
-  const int rows = 2 * c->D;
+  // Sector-aligned panels: consecutive sectors of at most 128 V rows are packed
+  // into one 128-row A panel with 32-row B panels over the group's rows; a
+  // larger sector gets its own 128-row A slices x 32-row B panels.
+  const int ns = int(c->sec_row.size());
   std::vector<std::pair<int, int>> tiles;
-  for (int i0 = 0; i0 < rows; i0 += 128) {
-    for (int j0 = 0; j0 < rows; j0 += 32) {
-      bool need = false;
-      for (size_t s = 0; s < c->sec_row.size() && !need; ++s) {
-        const int r0 = c->sec_row[s], r1 = r0 + 2 * c->basis.sector_dim[s];
-        if (r0 < i0 + 128 && r1 > i0 && r0 < j0 + 32 && r1 > j0) need = true;
-      }
-      if (need) tiles.push_back({i0, j0});
+  std::vector<TcSector> secs(ns);
+  for (int i = 0; i < ns;) {
+    const int r0 = c->sec_row[i], d0 = 2 * c->basis.sector_dim[i];
+    if (d0 > 128) {
+      const int na = (d0 + 127) / 128, nb = (d0 + 31) / 32;
+      const int t0 = int(tiles.size());
+      for (int x = 0; x < na; ++x)
+        for (int y = 0; y < nb; ++y) tiles.push_back({r0 + 128 * x, r0 + 32 * y});
+      secs[i] = {r0, c->basis.sector_dim[i], c->sec_goff[i], t0, r0, r0, nb};
+      ++i;
+      continue;
     }
+    int j = i, g1 = r0;
+    while (j < ns && 2 * c->basis.sector_dim[j] <= 128 &&
+           c->sec_row[j] + 2 * c->basis.sector_dim[j] - r0 <= 128) {
+      g1 = c->sec_row[j] + 2 * c->basis.sector_dim[j];
+      ++j;
+    }
+    const int nb = (g1 - r0 + 31) / 32;
+    const int t0 = int(tiles.size());
+    for (int y = 0; y < nb; ++y) tiles.push_back({r0, r0 + 32 * y});
+    for (int q = i; q < j; ++q)
+      secs[q] = {c->sec_row[q], c->basis.sector_dim[q], c->sec_goff[q], t0, r0, r0, nb};
+    i = j;
   }
   int sm = 148;
   int dev = 0;
@@ -355,37 +371,23 @@ int setup_tc(lemc_ctx* c) {
   cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, dev);
   const int nt = int(tiles.size());
   c->tc_ntiles = nt;
-  c->tc_npi = (rows + 127) / 128;
-  c->tc_npj = (rows + 31) / 32;
-  std::vector<int> tile_of(size_t(c->tc_npi) * c->tc_npj, -1);
-  for (int t = 0; t < nt; ++t) tile_of[(tiles[t].first / 128) * c->tc_npj + tiles[t].second / 32] = t;
-  LEMC_TRY(c->d_tile_of.alloc(tile_of.size()));
-  LEMC_CUDA(cudaMemcpy(c->d_tile_of.p, tile_of.data(), sizeof(int) * tile_of.size(),
-                       cudaMemcpyHostToDevice));
   c->tc_maxdim = 0;
   for (int d : c->basis.sector_dim) c->tc_maxdim = std::max(c->tc_maxdim, d);
-  c->tc_splits = std::max(1, std::min((sm + nt - 1) / nt, c->Wpad / 256));
+  // one wave: at most one job per SM
+  c->tc_splits = std::max(1, std::min(sm / std::max(1, nt), c->Wpad / 128));
   c->tc_tiles.clear();
-  for (int s = 0; s < c->tc_splits; ++s)
+  for (int sp = 0; sp < c->tc_splits; ++sp)
     for (int t = 0; t < nt; ++t)
-      c->tc_tiles.push_back({tiles[t].first, tiles[t].second, s, s * nt + t});
+      c->tc_tiles.push_back({tiles[t].first, tiles[t].second, sp, sp * nt + t});
   LEMC_TRY(c->d_tc_tiles.alloc(c->tc_tiles.size()));
   LEMC_CUDA(cudaMemcpy(c->d_tc_tiles.p, c->tc_tiles.data(), sizeof(TcTile) * c->tc_tiles.size(),
                        cudaMemcpyHostToDevice));
+  LEMC_TRY(c->d_tc_secs.alloc(ns));
+  LEMC_CUDA(cudaMemcpy(c->d_tc_secs.p, secs.data(), sizeof(TcSector) * ns, cudaMemcpyHostToDevice));
   const size_t slot = size_t(kTcSlot);
   LEMC_TRY(c->tc_partials.alloc(slot * c->tc_tiles.size()));
   LEMC_CUDA(cudaMemsetAsync(c->tc_partials.p, 0, sizeof(double) * slot * c->tc_tiles.size(),
                             c->stream));
-  std::vector<int32_t> dims(c->basis.sector_dim.begin(), c->basis.sector_dim.end());
-  std::vector<int32_t> goff(c->sec_goff.begin(), c->sec_goff.end());
-  std::vector<int32_t> srow(c->sec_row.begin(), c->sec_row.end());
-  const int ns = int(dims.size());
-  LEMC_TRY(c->d_sec_row.alloc(ns));
-  LEMC_TRY(c->d_sec_dim.alloc(ns));
-  LEMC_TRY(c->d_sec_goff.alloc(ns));
-  LEMC_CUDA(cudaMemcpy(c->d_sec_row.p, srow.data(), 4 * ns, cudaMemcpyHostToDevice));
-  LEMC_CUDA(cudaMemcpy(c->d_sec_dim.p, dims.data(), 4 * ns, cudaMemcpyHostToDevice));
-  LEMC_CUDA(cudaMemcpy(c->d_sec_goff.p, goff.data(), 4 * ns, cudaMemcpyHostToDevice));
   return LEMC_OK;
 }
 
@@ -393,10 +395,9 @@ int setup_tc(lemc_ctx* c) {
 // partials are zeroed afterwards).
 int flush_tc(lemc_ctx* c) {
   if (c->tc_tiles.empty()) return LEMC_OK;
-  LEMC_TRY(launch_gram_tc_reduce(c->tc_partials.p, c->d_tile_of.p, c->tc_npi, c->tc_npj,
-                                 c->tc_ntiles, c->tc_splits, c->d_sec_row.p, c->d_sec_dim.p,
-                                 c->d_sec_goff.p, int(c->sec_row.size()), c->tc_maxdim, c->gram.p,
-                                 c->gram_plane, c->stream));
+  LEMC_TRY(launch_gram_tc_reduce(c->tc_partials.p, c->d_tc_tiles.p, c->d_tc_secs.p,
+                                 int(c->sec_row.size()), c->tc_ntiles, c->tc_splits, c->tc_maxdim,
+                                 c->gram.p, c->gram_plane, c->stream));
   LEMC_CUDA(cudaMemsetAsync(c->tc_partials.p, 0, sizeof(double) * kTcSlot * c->tc_tiles.size(),
                             c->stream));
   return LEMC_OK;
@@ -530,11 +531,8 @@ int lemc_destroy(lemc_ctx* c) {
   c->rowacc.release();
   c->err.release();
   c->d_tc_tiles.release();
-  c->d_tile_of.release();
+  c->d_tc_secs.release();
   c->tc_partials.release();
-  c->d_sec_row.release();
-  c->d_sec_dim.release();
-  c->d_sec_goff.release();
   for (auto& e : c->ev)
     if (e) cudaEventDestroy(e);
   for (auto& e : c->pev) cudaEventDestroy(e);
@@ -751,7 +749,7 @@ int lemc_run(lemc_ctx* c, int n_sweeps, int measure) {
     LEMC_TRY(launch_basis(c->rec_p.p, c->W, c->K, c->N, c->prog.p, c->n_nodes, c->V.p, c->Wpad,
                           c->series.p + 8 * size_t(s), c->stream));
     if (c->profile) LEMC_CUDA(cudaEventRecord(c->pev[4 * s + 2], c->stream));
-    LEMC_TRY(gram_step(c, c->V.p, c->rec_w.p, c->W, c->cfg.gram_mode));
+    LEMC_TRY(gram_step(c, c->V.p, c->rec_w.p, c->Wpad, c->W, c->cfg.gram_mode));
     if (c->profile) LEMC_CUDA(cudaEventRecord(c->pev[4 * s + 3], c->stream));
     c->meas += 1;
   }
@@ -908,6 +906,7 @@ int lemc_sweep_device(void* pos, int W, int N, int m, float sigma, uint64_t seed
   a.rec_w = static_cast<float*>(rec_w);
   a.accepted = static_cast<uint32_t*>(accepted);
   a.W = W;
+  a.ldw = W;
   a.N = N;
   a.Npad = N;
   a.m = m;
@@ -952,7 +951,8 @@ int lemc_gram_device(lemc_ctx* c, const void* V, const void* rec_w, int W, int l
   cudaStream_t user = static_cast<cudaStream_t>(stream);
   LEMC_CUDA(cudaEventRecord(c->ev[2], user));
   LEMC_CUDA(cudaStreamWaitEvent(c->stream, c->ev[2], 0));
-  LEMC_TRY(gram_step(c, static_cast<const float*>(V), static_cast<const float*>(rec_w), W, mode));
+  LEMC_TRY(gram_step(c, static_cast<const float*>(V), static_cast<const float*>(rec_w), ldv, W,
+                     mode));
   LEMC_CUDA(cudaEventRecord(c->ev[3], c->stream));
   LEMC_CUDA(cudaStreamWaitEvent(user, c->ev[3], 0));
   return LEMC_OK;

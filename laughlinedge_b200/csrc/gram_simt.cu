@@ -21,7 +21,8 @@ constexpr int TS = 16;     // 16 x 16 output tile
 constexpr int CH = 64;     // walkers per staged chunk
 
 __global__ void __launch_bounds__(256)
-gram_simt_kernel(const float* __restrict__ V, int ldv, const float* __restrict__ rec_w, int W,
+gram_simt_kernel(const float* __restrict__ V, int ldv, const float* __restrict__ rec_w, int ldw,
+                 int W,
                  const GramJob* __restrict__ jobs, int n_splits, double* __restrict__ out0,
                  size_t plane0, double* __restrict__ out1, size_t plane1) {
   const GramJob jb = jobs[blockIdx.x];
@@ -54,11 +55,11 @@ gram_simt_kernel(const float* __restrict__ V, int ldv, const float* __restrict__
       const int wi = c0 + s;
       float v = 0.f;
       if (wi < wend) {
-        const float one = rec_w[(size_t)LEMC_W_ONE * W + wi];
+        const float one = rec_w[(size_t)LEMC_W_ONE * ldw + wi];
         if (jb.wset == 0)
-          v = (h == 0) ? one : one * rec_w[(size_t)(LEMC_W_ONE + h) * W + wi];
+          v = (h == 0) ? one : one * rec_w[(size_t)(LEMC_W_ONE + h) * ldw + wi];
         else
-          v = one * rec_w[(size_t)(p0 + h) * W + wi];
+          v = one * rec_w[(size_t)(p0 + h) * ldw + wi];
       }
       wt[h][s] = v;
     }
@@ -103,7 +104,7 @@ constexpr int NROWACC = 13;
 
 __global__ void __launch_bounds__(256)
 row_accumulate_kernel(const float* __restrict__ V, int ldv, const float* __restrict__ rec_w,
-                      int W, const int32_t* __restrict__ row_first, int D,
+                      int ldw, const int32_t* __restrict__ row_first, int D,
                       const int32_t* __restrict__ row_re, const int32_t* __restrict__ row_im,
                       double* __restrict__ acc_out) {
   const int a = blockIdx.x;
@@ -122,12 +123,12 @@ row_accumulate_kernel(const float* __restrict__ V, int ldv, const float* __restr
       // v_b / v_a = v_b conj(v_a) / |v_a|^2
       const double rr = (vbr * var + vbi * vai) / den;
       const double ri = (vbi * var - vbr * vai) / den;
-      const double one = rec_w[(size_t)LEMC_W_ONE * W + w];
-      const double h2 = rec_w[(size_t)LEMC_W_R2 * W + w];
-      const double h4 = rec_w[(size_t)LEMC_W_R4 * W + w];
-      const double hc = rec_w[(size_t)LEMC_W_COS * W + w];
-      const double hs = rec_w[(size_t)LEMC_W_SIN * W + w];
-      const double hu = rec_w[(size_t)LEMC_W_USER * W + w];
+      const double one = rec_w[(size_t)LEMC_W_ONE * ldw + w];
+      const double h2 = rec_w[(size_t)LEMC_W_R2 * ldw + w];
+      const double h4 = rec_w[(size_t)LEMC_W_R4 * ldw + w];
+      const double hc = rec_w[(size_t)LEMC_W_COS * ldw + w];
+      const double hs = rec_w[(size_t)LEMC_W_SIN * ldw + w];
+      const double hu = rec_w[(size_t)LEMC_W_USER * ldw + w];
       acc[0] += one * rr;
       acc[1] += one * ri;
       acc[2] += one * (rr * rr + ri * ri);
@@ -158,22 +159,23 @@ row_accumulate_kernel(const float* __restrict__ V, int ldv, const float* __restr
 
 }  // namespace
 
-int launch_gram_simt(const float* V, int ldv, const float* rec_w, int W, const GramJob* jobs,
+int launch_gram_simt(const float* V, int ldv, const float* rec_w, int ldw, int W, const GramJob* jobs,
                      int n_jobs, int n_splits, double* out0, size_t plane0, double* out1,
                      size_t plane1, cudaStream_t st) {
   if (n_jobs <= 0) return LEMC_OK;
   dim3 grid(n_jobs, n_splits);
-  gram_simt_kernel<<<grid, 256, 0, st>>>(V, ldv, rec_w, W, jobs, n_splits, out0, plane0, out1,
+  gram_simt_kernel<<<grid, 256, 0, st>>>(V, ldv, rec_w, ldw, W, jobs, n_splits, out0, plane0, out1,
                                          plane1);
   return cudaPeekAtLastError() == cudaSuccess ? LEMC_OK : LEMC_ERR_CUDA;
 }
 
-int launch_row_accumulate(const float* V, int ldv, const float* rec_w, int W,
+int launch_row_accumulate(const float* V, int ldv, const float* rec_w, int ldw, int W,
                           const int32_t* row_first, int n_rows, int D, const int32_t* row_re,
                           const int32_t* row_im, double* acc, cudaStream_t st) {
   if (n_rows <= 0 || D <= 0) return LEMC_OK;
+  (void)W;
   dim3 grid(n_rows, (D + 31) / 32);
-  row_accumulate_kernel<<<grid, 256, 0, st>>>(V, ldv, rec_w, W, row_first, D, row_re, row_im,
+  row_accumulate_kernel<<<grid, 256, 0, st>>>(V, ldv, rec_w, ldw, row_first, D, row_re, row_im,
                                               acc);
   return cudaPeekAtLastError() == cudaSuccess ? LEMC_OK : LEMC_ERR_CUDA;
 }

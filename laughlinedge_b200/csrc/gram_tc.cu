@@ -2,26 +2,36 @@
 //
 // For every tile job (A panel of 128 V rows, B panel of 32 V rows, walker
 // split) the kernel accumulates
-//   D[r][h*32 + c] = sum_w V[row0+r][w] * W_h(w) * V[col0+c][w],   h = 0,1,2
+//   D[r][h*32 + c] = sum_w V[a0+r][w] * W_h(w) * V[b0+c][w],   h = 0,1,2
 // with W_0 = w1, W_1 = w1 sum|z|^2, W_2 = w1 sum|z|^4: one M=128 x N=96 MMA
 // produces the S, H2 and H4 blocks at once.  Complex Gram entries are
 // recovered from the real products of the [Re; Im] row planes afterwards.
 //
 // Precision: each FP32 operand x is split x = hi + lo with hi = bf16(x),
 // lo = bf16(x - hi) (kind::f16) or hi = x truncated to TF32, lo = x - hi
-// (kind::tf32).  The products hi*hi + hi*lo + lo*hi (+ lo*lo) accumulate in
-// FP32 in tensor memory, hi*hi in one accumulator and the (2^-8 smaller)
-// correction products in a second one, so the FP32 rounding of the corrections
-// does not reach the result; every `flush_every` K-chunks the epilogue warps
-// move both accumulators into an FP64 tile in shared memory (double-buffered
-// TMEM so the MMAs continue meanwhile); at the end the FP64 tile is added to
-// the job's private FP64 slot in global memory.
+// (kind::tf32).  hi*hi accumulates in one FP32 tensor-memory accumulator and
+// the correction products hi*lo + lo*hi (+ lo*lo) in a second one, so their
+// FP32 rounding stays 2^-8 (BF16) or 2^-11 (TF32) below the result.  Every
+// `flush_every` K-chunks the epilogue warps add both accumulators into
+// compensated FP32 register sums (Knuth's TwoSum: the rounding error of every
+// addition is carried exactly in a second FP32 word, so the running sum keeps
+// ~48 bits however many flushes it takes; double-buffered TMEM lets the MMAs
+// continue meanwhile).  At the end each job adds sum + compensation, in FP64,
+// to its private slot in global memory.
 //
-// Warp roles (288 threads): warps 0-3 producers (global FP32 -> split
-// operands, 128B-swizzled K-major shared memory), warps 4-7 epilogue (TMEM
-// lane quarter = warp % 4), warp 8 allocates TMEM and one lane issues the
-// MMAs.  Every mbarrier wait is bounded in time; on expiry the kernel records
-// LEMC_ERR_TIMEOUT in the error word and unwinds.
+// Pipeline (576 threads, one CTA per SM):
+//   warp 17      loader: three tiled TMA loads per K-chunk (A panel 128 x KC,
+//                B panel 32 x KC, weight planes 3 x KC; rows past the end are
+//                zero-filled by the TMA unit) into a ring of raw FP32 stages;
+//   warps 12-15  converters: raw FP32 -> weighted, split hi/lo operands in
+//                128-byte-swizzled K-major layout (two operand stages);
+//   warp 16      allocates 512 TMEM columns, one lane issues tcgen05.mma;
+//   warps 0-11   epilogue: TMEM lane quarter = warp % 4, column third =
+//                warp / 4, 32 compensated FP32 accumulators per thread.
+// No load uses cluster multicast; every source is this GPU's own memory.
+// Every mbarrier wait is bounded in time; on expiry the kernel records
+// LEMC_ERR_TIMEOUT in the error word, skips its output and unwinds.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -34,25 +44,39 @@ namespace {
 constexpr int kM = 128;            // A panel rows (MMA M)
 constexpr int kNB = 32;            // B panel rows per weight
 constexpr int kN = 3 * kNB;        // MMA N
-constexpr int kRowBytes = 128;     // one swizzle-128B row = one K-chunk
-constexpr int kATileBytes = kM * kRowBytes;   // 16 KB
-constexpr int kBTileBytes = kN * kRowBytes;   // 12 KB
-constexpr int kStageBytes = 2 * kATileBytes + 2 * kBTileBytes;  // hi + lo
-constexpr int kStages = 2;
-constexpr int kAccLd = kN + 1;     // FP64 accumulator row stride (doubles)
-constexpr int kThreads = 288;
-constexpr int kTmemCols = 512;     // two buffers x (hi*hi accumulator, correction accumulator)
-constexpr int kBufCols = 256;      // buffer b: hi*hi at b*256, corrections at b*256 + 128
+constexpr int kOpRowBytes = 128;   // one swizzle-128B row of split operands
+constexpr int kATileBytes = kM * kOpRowBytes;  // 16 KB
+constexpr int kBTileBytes = kN * kOpRowBytes;  // 12 KB
+constexpr int kOpStageBytes = 2 * kATileBytes + 2 * kBTileBytes;  // hi + lo
+constexpr int kOpStages = 2;
+constexpr int kEpiWarps = 12;
+constexpr int kConvWarp0 = 12;
+constexpr int kMmaWarp = 16;
+constexpr int kLoadWarp = 17;
+constexpr int kThreads = 18 * 32;
+constexpr int kTmemCols = 512;     // 2 buffers x (hi*hi at +0, corrections at +128)
+constexpr int kBufCols = 256;
 constexpr long long kWaitCycles = 4000000000LL;  // ~2 s at 1.9 GHz
 
+template <bool TF32>
+struct Cfg {
+  static constexpr int KC = TF32 ? 32 : 64;           // samples per K-chunk
+  static constexpr int RAW_ROW = KC * 4;              // bytes of one raw FP32 row segment
+  static constexpr int RAW_W = 3 * KC * 4;            // weight planes of one chunk
+  static constexpr int RAW_STAGE = (kM + kNB) * RAW_ROW + RAW_W;
+  static constexpr int RAW_STAGES = TF32 ? 4 : 2;
+};
+
+template <bool TF32>
 struct Smem {
-  // operand stages first (1024-byte aligned by construction)
-  uint8_t stage[kStages][kStageBytes];
-  double acc[kM * kAccLd];
-  uint64_t full[kStages];
-  uint64_t empty[kStages];
-  uint64_t tfull[2];
-  uint64_t tempty[2];
+  uint8_t op[kOpStages][kOpStageBytes];  // 1024-aligned operand stages
+  uint8_t raw[Cfg<TF32>::RAW_STAGES][Cfg<TF32>::RAW_STAGE];
+  uint64_t raw_full[Cfg<TF32>::RAW_STAGES];
+  uint64_t raw_empty[Cfg<TF32>::RAW_STAGES];
+  uint64_t op_full[kOpStages];
+  uint64_t op_empty[kOpStages];
+  uint64_t acc_full[2];
+  uint64_t acc_empty[2];
   uint64_t done;
   uint32_t tmem_base;
   int abort_flag;
@@ -70,6 +94,12 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
+__device__ __forceinline__ void mbar_arrive_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
 __device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(
@@ -82,14 +112,14 @@ __device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Bounded wait; returns false (and raises the CTA abort flag and the global
-// error word) when the phase does not complete in time or another role gave up.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, Smem* sm, int* err) {
+// Bounded wait; returns false (raising the CTA abort flag and the global error
+// word) when the phase does not complete in time or another role gave up.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* abort_flag, int* err) {
   const long long t0 = clock64();
   while (!mbar_try(bar, parity)) {
-    if (*(volatile int*)&sm->abort_flag) return false;
+    if (*(volatile int*)abort_flag) return false;
     if (clock64() - t0 > kWaitCycles) {
-      *(volatile int*)&sm->abort_flag = 1;
+      *(volatile int*)abort_flag = 1;
       if (err) atomicExch(err, LEMC_ERR_TIMEOUT);
       return false;
     }
@@ -97,15 +127,25 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, Smem* 
   return true;
 }
 
+// Tiled 2D TMA load (no multicast) completing on an mbarrier transaction count.
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y,
+                                            uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+
 // UMMA shared-memory descriptor: K-major, 128-byte swizzle, 8-row groups
-// 1024 bytes apart (SBO), version 1 (sm_100).
+// 1024 bytes apart (SBO), LBO 1 (unused for swizzled K-major), version 1.
 __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
   uint64_t d = 0;
   d |= uint64_t((saddr >> 4) & 0x3FFF);
-  d |= uint64_t(1) << 16;                 // LBO (unused for swizzled K-major)
-  d |= uint64_t((1024 >> 4) & 0x3FFF) << 32;  // SBO
-  d |= uint64_t(1) << 46;                 // descriptor version
-  d |= uint64_t(2) << 61;                 // SWIZZLE_128B
+  d |= uint64_t(1) << 16;
+  d |= uint64_t((1024 >> 4) & 0x3FFF) << 32;
+  d |= uint64_t(1) << 46;
+  d |= uint64_t(2) << 61;
   return d;
 }
 
@@ -149,21 +189,17 @@ __device__ __forceinline__ void fence_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
-  uint32_t r[32];
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t* r) {
   asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
         "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
-        "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
-        "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        "=r"(r[14]), "=r"(r[15])
       : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld() {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
 // byte offset of 16-byte chunk `c` of row `r` in a 128B-swizzled K-major tile
@@ -171,7 +207,6 @@ __device__ __forceinline__ uint32_t sw128_off(int r, int c) {
   return uint32_t((r >> 3) * 1024 + (r & 7) * 128 + ((c ^ (r & 7)) << 4));
 }
 
-// split 8 consecutive FP32 values into bf16 hi and lo 16-byte chunks
 __device__ __forceinline__ void split_bf16x8(const float* x, uint4& hi, uint4& lo) {
   uint32_t h[4], l[4];
 #pragma unroll
@@ -186,7 +221,6 @@ __device__ __forceinline__ void split_bf16x8(const float* x, uint4& hi, uint4& l
   lo = make_uint4(l[0], l[1], l[2], l[3]);
 }
 
-// split 4 FP32 values into TF32 hi (truncated) and FP32 lo = x - hi
 __device__ __forceinline__ void split_tf32x4(const float* x, uint4& hi, uint4& lo) {
   uint32_t h[4], l[4];
 #pragma unroll
@@ -203,8 +237,8 @@ struct TcArgs {
   const float* V;
   int ldv;
   int total_rows;
-  const float* rec_w;
-  int W;
+  const float* rec_w;   // weight planes, stride ldw (256-byte aligned rows)
+  int ldw;
   const TcTile* tiles;
   double* partials;
   int n_chunks_total;   // K-chunks over the padded walker range
@@ -215,16 +249,19 @@ struct TcArgs {
 };
 
 template <bool TF32>
-__global__ void __launch_bounds__(kThreads, 1) gram_tc_kernel(const TcArgs a) {
-  extern __shared__ __align__(1024) uint8_t smem_raw[];
-  // align the Smem struct to 1024 bytes for the swizzle atoms
-  Smem* sm = reinterpret_cast<Smem*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-
-  constexpr int KC = TF32 ? 32 : 64;          // samples per K-chunk (one 128-byte row)
-  constexpr int EPC = TF32 ? 4 : 8;           // elements per 16-byte chunk
-  constexpr int KSTEP_BYTES = 32;             // one MMA consumes 32 bytes of K
-  constexpr int NKSTEP = kRowBytes / KSTEP_BYTES;
+__global__ void __launch_bounds__(kThreads, 1)
+gram_tc_kernel(const TcArgs a, const __grid_constant__ CUtensorMap tmA,
+               const __grid_constant__ CUtensorMap tmB, const __grid_constant__ CUtensorMap tmW) {
+  using C = Cfg<TF32>;
+  constexpr int KC = C::KC;
+  constexpr int EPC = TF32 ? 4 : 8;          // elements per 16-byte operand chunk
+  constexpr int NKSTEP = kOpRowBytes / 32;   // one MMA consumes 32 bytes of K
   constexpr uint32_t IDESC = make_idesc(TF32 ? 2u : 1u);
+  constexpr int RS = C::RAW_STAGES;
+
+  extern __shared__ __align__(1024) uint8_t smem_raw[];
+  Smem<TF32>* sm = reinterpret_cast<Smem<TF32>*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
 
   const TcTile tile = a.tiles[blockIdx.x];
   const int warp = threadIdx.x >> 5;
@@ -234,60 +271,78 @@ __global__ void __launch_bounds__(kThreads, 1) gram_tc_kernel(const TcArgs a) {
   const int c_end = min(a.n_chunks_total, c_beg + per);
   const int nch = max(0, c_end - c_beg);
   const int F = a.flush_every;
-  const int nint = (nch + F - 1) / F;  // accumulation intervals
+  const int nint = (nch + F - 1) / F;
 
   if (threadIdx.x == 0) {
-    for (int s = 0; s < kStages; ++s) {
-      mbar_init(&sm->full[s], 128);
-      mbar_init(&sm->empty[s], 1);
+    for (int s = 0; s < RS; ++s) {
+      mbar_init(&sm->raw_full[s], 1);
+      mbar_init(&sm->raw_empty[s], 128);
+    }
+    for (int s = 0; s < kOpStages; ++s) {
+      mbar_init(&sm->op_full[s], 128);
+      mbar_init(&sm->op_empty[s], 1);
     }
     for (int b = 0; b < 2; ++b) {
-      mbar_init(&sm->tfull[b], 1);
-      mbar_init(&sm->tempty[b], 128);
+      mbar_init(&sm->acc_full[b], 1);
+      mbar_init(&sm->acc_empty[b], kEpiWarps * 32);
     }
     mbar_init(&sm->done, 1);
     sm->abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (warp == 8) {
+  if (warp == kMmaWarp) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      smem_u32(&sm->tmem_base)),
                  "r"(kTmemCols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
-  if (warp >= 4 && warp < 8) {
-    for (int i = threadIdx.x - 128; i < kM * kAccLd; i += 128) sm->acc[i] = 0.0;
-  }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = sm->tmem_base;
+  int* abort_flag = &sm->abort_flag;
 
-  if (warp < 4) {
-    // ------------------------------ producers ------------------------------
-    const int t = threadIdx.x;
+  if (warp == kLoadWarp) {
+    // ------------------------------- loader --------------------------------
+    if (lane == 0) {
+      const uint32_t tx_bytes = uint32_t(C::RAW_STAGE);
+      for (int c = 0; c < nch; ++c) {
+        const int s = c % RS;
+        if (!mbar_wait(&sm->raw_empty[s], (uint32_t(c / RS) & 1u) ^ 1u, abort_flag, a.err)) break;
+        const int k0 = (c_beg + c) * KC;
+        uint8_t* dst = sm->raw[s];
+        mbar_arrive_tx(&sm->raw_full[s], tx_bytes);
+        tma_load_2d(dst, &tmA, k0, tile.row0, &sm->raw_full[s]);
+        tma_load_2d(dst + kM * C::RAW_ROW, &tmB, k0, tile.col0, &sm->raw_full[s]);
+        tma_load_2d(dst + (kM + kNB) * C::RAW_ROW, &tmW, k0, 0, &sm->raw_full[s]);
+      }
+    }
+    __syncwarp();
+  } else if (warp >= kConvWarp0 && warp < kConvWarp0 + 4) {
+    // ------------------------------ converters -----------------------------
+    const int t = threadIdx.x - kConvWarp0 * 32;
     for (int c = 0; c < nch; ++c) {
-      const int s = c % kStages;
-      const uint32_t ph = uint32_t(c / kStages) & 1u;
-      if (!mbar_wait(&sm->empty[s], ph ^ 1u, sm, a.err)) break;
-      uint8_t* st = sm->stage[s];
+      const int rs = c % RS, os = c % kOpStages;
+      if (!mbar_wait(&sm->raw_full[rs], uint32_t(c / RS) & 1u, abort_flag, a.err)) break;
+      if (!mbar_wait(&sm->op_empty[os], (uint32_t(c / kOpStages) & 1u) ^ 1u, abort_flag, a.err)) break;
+      const uint8_t* raw = sm->raw[rs];
+      const float* rw = reinterpret_cast<const float*>(raw + (kM + kNB) * C::RAW_ROW);
+      uint8_t* st = sm->op[os];
       uint8_t* a_hi = st;
       uint8_t* a_lo = st + kATileBytes;
       uint8_t* b_hi = st + 2 * kATileBytes;
-      uint8_t* b_lo = st + 2 * kATileBytes + kBTileBytes;
-      const int k0 = (c_beg + c) * KC;
-      // A: 128 rows x 8 chunks, unweighted
+      uint8_t* b_lo = b_hi + kBTileBytes;
+      // A: 128 rows x 8 operand chunks, unweighted
 #pragma unroll 2
       for (int q = 0; q < 8; ++q) {
         const int id = q * 128 + t;
         const int r = id >> 3, ch = id & 7;
-        const int row = tile.row0 + r;
         float x[EPC];
-        if (row < a.total_rows) {
-          const float4* src = reinterpret_cast<const float4*>(a.V + (size_t)row * a.ldv + k0 + ch * EPC);
+        if (tile.row0 + r < a.total_rows) {
+          const float4* src = reinterpret_cast<const float4*>(raw + r * C::RAW_ROW + ch * EPC * 4);
 #pragma unroll
           for (int v = 0; v < EPC / 4; ++v) {
-            const float4 f = __ldg(src + v);
+            const float4 f = src[v];
             x[4 * v] = f.x; x[4 * v + 1] = f.y; x[4 * v + 2] = f.z; x[4 * v + 3] = f.w;
           }
         } else {
@@ -300,39 +355,34 @@ __global__ void __launch_bounds__(kThreads, 1) gram_tc_kernel(const TcArgs a) {
         *reinterpret_cast<uint4*>(a_hi + off) = hi;
         *reinterpret_cast<uint4*>(a_lo + off) = lo;
       }
-      // B: 32 rows x 8 chunks, three weight planes
+      // B: 32 rows x 8 operand chunks x 3 weight planes
 #pragma unroll 1
       for (int q = 0; q < 2; ++q) {
         const int id = q * 128 + t;
         const int r = id >> 3, ch = id & 7;
-        const int row = tile.col0 + r;
-        float x[EPC], w0[EPC], w1[EPC], w2[EPC];
-        const int kk = k0 + ch * EPC;
-#pragma unroll
-        for (int e = 0; e < EPC; ++e) {
-          const int wi = kk + e;
-          const bool ok = (wi < a.W);
-          const float one = ok ? __ldg(a.rec_w + (size_t)LEMC_W_ONE * a.W + wi) : 0.f;
-          w0[e] = one;
-          w1[e] = ok ? one * __ldg(a.rec_w + (size_t)LEMC_W_R2 * a.W + wi) : 0.f;
-          w2[e] = ok ? one * __ldg(a.rec_w + (size_t)LEMC_W_R4 * a.W + wi) : 0.f;
-        }
-        if (row < a.total_rows) {
-          const float4* src = reinterpret_cast<const float4*>(a.V + (size_t)row * a.ldv + kk);
+        float x[EPC];
+        if (tile.col0 + r < a.total_rows) {
+          const float4* src = reinterpret_cast<const float4*>(raw + (kM + r) * C::RAW_ROW + ch * EPC * 4);
 #pragma unroll
           for (int v = 0; v < EPC / 4; ++v) {
-            const float4 f = __ldg(src + v);
+            const float4 f = src[v];
             x[4 * v] = f.x; x[4 * v + 1] = f.y; x[4 * v + 2] = f.z; x[4 * v + 3] = f.w;
           }
         } else {
 #pragma unroll
           for (int e = 0; e < EPC; ++e) x[e] = 0.f;
         }
+        const float* w0 = rw + ch * EPC;
+        const float* w1 = rw + KC + ch * EPC;
+        const float* w2 = rw + 2 * KC + ch * EPC;
 #pragma unroll
         for (int h = 0; h < 3; ++h) {
           float y[EPC];
 #pragma unroll
-          for (int e = 0; e < EPC; ++e) y[e] = x[e] * (h == 0 ? w0[e] : (h == 1 ? w1[e] : w2[e]));
+          for (int e = 0; e < EPC; ++e) {
+            const float one = w0[e];
+            y[e] = x[e] * (h == 0 ? one : (h == 1 ? one * w1[e] : one * w2[e]));
+          }
           uint4 hi, lo;
           if (TF32) split_tf32x4(y, hi, lo); else split_bf16x8(y, hi, lo);
           const uint32_t off = sw128_off(h * kNB + r, ch);
@@ -341,79 +391,101 @@ __global__ void __launch_bounds__(kThreads, 1) gram_tc_kernel(const TcArgs a) {
         }
       }
       fence_async_smem();
-      mbar_arrive(&sm->full[s]);
+      mbar_arrive(&sm->op_full[os]);
+      mbar_arrive(&sm->raw_empty[rs]);
     }
-  } else if (warp < 8) {
-    // ------------------------------ epilogue -------------------------------
+  } else if (warp == kMmaWarp) {
+    // ------------------------------ MMA issuer -----------------------------
+    if (lane == 0) {
+      bool ok = true;
+      for (int c = 0; c < nch && ok; ++c) {
+        const int s = c % kOpStages;
+        const int q = c / F;
+        const int b = q & 1;
+        if (c % F == 0) {
+          if (!mbar_wait(&sm->acc_empty[b], (uint32_t(q >> 1) & 1u) ^ 1u, abort_flag, a.err)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+        }
+        if (!mbar_wait(&sm->op_full[s], uint32_t(c / kOpStages) & 1u, abort_flag, a.err)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t base = smem_u32(sm->op[s]);
+        const uint32_t ahi = base, alo = base + kATileBytes;
+        const uint32_t bhi = base + 2 * kATileBytes, blo = bhi + kBTileBytes;
+        const uint32_t d = tmem + uint32_t(b * kBufCols);
+        const uint32_t dc = d + 128u;
+#pragma unroll
+        for (int ks = 0; ks < NKSTEP; ++ks) {
+          const uint32_t o = ks * 32;
+          const uint32_t first = (c % F == 0 && ks == 0) ? 0u : 1u;
+          mma<TF32>(d, sw128_desc(ahi + o), sw128_desc(bhi + o), IDESC, first);
+          mma<TF32>(dc, sw128_desc(ahi + o), sw128_desc(blo + o), IDESC, first);
+          mma<TF32>(dc, sw128_desc(alo + o), sw128_desc(bhi + o), IDESC, 1u);
+          if (a.passes > 3) mma<TF32>(dc, sw128_desc(alo + o), sw128_desc(blo + o), IDESC, 1u);
+        }
+        umma_commit(&sm->op_empty[s]);
+        if (c % F == F - 1 || c == nch - 1) umma_commit(&sm->acc_full[b]);
+      }
+      if (nch > 0) {
+        // every issued MMA must retire before TMEM is released
+        umma_commit(&sm->done);
+        mbar_wait(&sm->done, 0u, abort_flag, a.err);
+      }
+    }
+    __syncwarp();
+  } else if (warp < kEpiWarps) {
+    // ------------------------------- epilogue ------------------------------
     const int quarter = warp & 3;
-    const int row = quarter * 32 + lane;
+    const int third = warp >> 2;
+    float sum[32], cmp[32];
+#pragma unroll
+    for (int i = 0; i < 32; ++i) {
+      sum[i] = 0.f;
+      cmp[i] = 0.f;
+    }
+    const uint32_t lane_base = uint32_t(quarter * 32) << 16;
     for (int q = 0; q < nint; ++q) {
       const int b = q & 1;
-      if (!mbar_wait(&sm->tfull[b], uint32_t(q >> 1) & 1u, sm, a.err)) break;
+      if (!mbar_wait(&sm->acc_full[b], uint32_t(q >> 1) & 1u, abort_flag, a.err)) break;
       tc_fence_after();
-#pragma unroll 1
-      for (int cc = 0; cc < kN / 32; ++cc) {
-        float v[32], u[32];
-        const uint32_t ta = tmem + (uint32_t(quarter * 32) << 16) + uint32_t(b * kBufCols + cc * 32);
-        tmem_ld32(ta, v);
-        tmem_ld32(ta + 128, u);
-        double* dst = sm->acc + row * kAccLd + cc * 32;
+      const uint32_t ta = tmem + lane_base + uint32_t(b * kBufCols + third * 32);
 #pragma unroll
-        for (int i = 0; i < 32; ++i) dst[i] += double(v[i]) + double(u[i]);
+      for (int half = 0; half < 2; ++half) {
+        uint32_t hv[16], cv[16];
+        tmem_ld16(ta + half * 16, hv);
+        tmem_ld16(ta + 128 + half * 16, cv);
+        tmem_wait_ld();
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+          const int k = half * 16 + i;
+          const float y = __uint_as_float(hv[i]) + __uint_as_float(cv[i]);
+          // TwoSum: t + e == sum + y exactly
+          const float t = sum[k] + y;
+          const float z = t - sum[k];
+          const float e = (sum[k] - (t - z)) + (y - z);
+          sum[k] = t;
+          cmp[k] += e;
+        }
       }
       tc_fence_before();
-      mbar_arrive(&sm->tempty[b]);
+      mbar_arrive(&sm->acc_empty[b]);
     }
-  } else if (lane == 0) {
-    // ------------------------------ MMA issuer -----------------------------
-    bool ok = true;
-    for (int c = 0; c < nch && ok; ++c) {
-      const int s = c % kStages;
-      const int q = c / F;
-      const int b = q & 1;
-      if (c % F == 0) {
-        // the epilogue must have drained this accumulator buffer
-        if (!mbar_wait(&sm->tempty[b], (uint32_t(q >> 1) & 1u) ^ 1u, sm, a.err)) { ok = false; break; }
-        tc_fence_after();
-      }
-      if (!mbar_wait(&sm->full[s], uint32_t(c / kStages) & 1u, sm, a.err)) { ok = false; break; }
-      tc_fence_after();
-      const uint32_t base = smem_u32(sm->stage[s]);
-      const uint32_t ahi = base, alo = base + kATileBytes;
-      const uint32_t bhi = base + 2 * kATileBytes, blo = bhi + kBTileBytes;
-      const uint32_t d = tmem + uint32_t(b * kBufCols);   // hi*hi
-      const uint32_t dc = d + 128u;                          // corrections
+    if (!*(volatile int*)abort_flag && nint > 0) {
+      double* slot = a.partials + (size_t)tile.slot * (kM * kN) +
+                     (size_t)(quarter * 32 + lane) * kN + third * 32;
 #pragma unroll
-      for (int ks = 0; ks < NKSTEP; ++ks) {
-        const uint32_t o = ks * KSTEP_BYTES;
-        const uint32_t first = (c % F == 0 && ks == 0) ? 0u : 1u;
-        mma<TF32>(d, sw128_desc(ahi + o), sw128_desc(bhi + o), IDESC, first);
-        mma<TF32>(dc, sw128_desc(ahi + o), sw128_desc(blo + o), IDESC, first);
-        mma<TF32>(dc, sw128_desc(alo + o), sw128_desc(bhi + o), IDESC, 1u);
-        if (a.passes > 3) mma<TF32>(dc, sw128_desc(alo + o), sw128_desc(blo + o), IDESC, 1u);
-      }
-      umma_commit(&sm->empty[s]);
-      if (c % F == F - 1 || c == nch - 1) umma_commit(&sm->tfull[b]);
-    }
-    if (nch > 0) {
-      // all issued MMAs must retire before TMEM is released
-      umma_commit(&sm->done);
-      mbar_wait(&sm->done, 0u, sm, a.err);
+      for (int i = 0; i < 32; ++i) slot[i] += double(sum[i]) + double(cmp[i]);
     }
   }
 
-  __syncthreads();
-  // epilogue warps add the FP64 tile to the job's private slot
-  if (warp >= 4 && warp < 8 && !sm->abort_flag) {
-    double* slot = a.partials + (size_t)tile.slot * (kM * kN);
-    for (int i = threadIdx.x - 128; i < kM * kN; i += 128) {
-      const int r = i / kN, cidx = i % kN;
-      slot[i] += sm->acc[r * kAccLd + cidx];
-    }
-  }
   tc_fence_before();
   __syncthreads();
-  if (warp == 8) {
+  if (warp == kMmaWarp) {
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
   }
@@ -422,90 +494,134 @@ __global__ void __launch_bounds__(kThreads, 1) gram_tc_kernel(const TcArgs a) {
 // Fold the partial slots into the per-sector complex Gram planes:
 //   G_h[a][b] += sum_splits [C(re a, re b) + C(im a, im b)]
 //              + i [C(re a, im b) - C(im a, re b)]
+// with C(r1, r2) read from the tile that covers A row r1 and B row r2.  Each
+// sector knows its tiles: first tile index, A/B row origins and the number
+// of B panels (TcSector).
 __global__ void gram_tc_reduce_kernel(const double* __restrict__ partials,
-                                      const int* __restrict__ tile_of, int n_pi, int n_pj,
-                                      int n_tiles, int n_splits, const int32_t* __restrict__ sec_row,
-                                      const int32_t* __restrict__ sec_dim,
-                                      const int32_t* __restrict__ sec_goff, int n_sec,
-                                      double* __restrict__ gram, size_t plane) {
+                                      const TcTile* __restrict__ tiles,
+                                      const TcSector* __restrict__ secs, int n_sec, int n_tiles,
+                                      int n_splits, double* __restrict__ gram, size_t plane) {
   const int s = blockIdx.y;
   if (s >= n_sec) return;
-  const int D = sec_dim[s];
+  const TcSector sc = secs[s];
+  const int D = sc.dim;
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= D * D) return;
   const int a = idx / D, b = idx % D;
-  const int r0 = sec_row[s];
   auto C = [&](int r1, int r2, int h) {
-    const int t = tile_of[(r1 / kM) * n_pj + (r2 / kNB)];
+    const int t = sc.tile0 + ((r1 - sc.a_base) / kM) * sc.n_bpanels + (r2 - sc.b_base) / kNB;
     double v = 0.0;
-    if (t < 0) return v;
+    if (t < 0 || t >= n_tiles) return v;
+    const TcTile tl = tiles[t];
+    const int i = r1 - tl.row0, j = r2 - tl.col0;
+    if (i < 0 || i >= kM || j < 0 || j >= kNB) return v;
     for (int sp = 0; sp < n_splits; ++sp) {
       const double* slot = partials + (size_t)(sp * n_tiles + t) * (kM * kN);
-      v += slot[(r1 % kM) * kN + h * kNB + (r2 % kNB)];
+      v += slot[i * kN + h * kNB + j];
     }
     return v;
   };
-  const int ra = r0 + a, ia = r0 + D + a, rb = r0 + b, ib = r0 + D + b;
+  const int ra = sc.row + a, ia = sc.row + D + a, rb = sc.row + b, ib = sc.row + D + b;
   for (int h = 0; h < 3; ++h) {
     const double re = C(ra, rb, h) + C(ia, ib, h);
     const double im = C(ra, ib, h) - C(ia, rb, h);
-    const size_t o = 2 * ((size_t)sec_goff[s] + (size_t)a * D + b) + 2 * plane * h;
+    const size_t o = 2 * ((size_t)sc.goff + (size_t)a * D + b) + 2 * plane * h;
     gram[o] += re;
     gram[o + 1] += im;
   }
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// dependency on libcuda).
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                   const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                   const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
+// 2D FP32 map over a row-major [rows][ld] array, box = box_x samples x box_y rows,
+// no swizzle, rows past `rows` read as zero.
+bool make_map(CUtensorMap* m, const float* base, int ld, int rows, int box_x, int box_y) {
+  EncodeTiledFn fn = encode_fn();
+  if (!fn) return false;
+  const cuuint64_t dims[2] = {cuuint64_t(ld), cuuint64_t(rows)};
+  const cuuint64_t strides[1] = {cuuint64_t(ld) * sizeof(float)};
+  const cuuint32_t box[2] = {cuuint32_t(box_x), cuuint32_t(box_y)};
+  const cuuint32_t estr[2] = {1, 1};
+  return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(base), dims, strides, box,
+            estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <bool TF32>
+int launch_t(const TcArgs& a, int n_jobs, cudaStream_t st) {
+  const size_t smem = sizeof(Smem<TF32>) + 1024;
+  if (smem > 227 * 1024) return LEMC_ERR_CAPACITY;
+  constexpr int KC = Cfg<TF32>::KC;
+  CUtensorMap tmA, tmB, tmW;
+  if (!make_map(&tmA, a.V, a.ldv, a.total_rows, KC, kM) ||
+      !make_map(&tmB, a.V, a.ldv, a.total_rows, KC, kNB) ||
+      !make_map(&tmW, a.rec_w, a.ldw, 3, KC, 3))
+    return LEMC_ERR_CUDA;
+  if (cudaFuncSetAttribute(gram_tc_kernel<TF32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           int(smem)) != cudaSuccess)
+    return LEMC_ERR_CUDA;
+  gram_tc_kernel<TF32><<<n_jobs, kThreads, smem, st>>>(a, tmA, tmB, tmW);
+  return cudaPeekAtLastError() == cudaSuccess ? LEMC_OK : LEMC_ERR_CUDA;
+}
+
 }  // namespace
 
-int launch_gram_tc_rows(const float* V, int ldv, int total_rows, const float* rec_w, int W,
+int launch_gram_tc_rows(const float* V, int ldv, int total_rows, const float* rec_w, int ldw,
                         int Wpad, const TcTile* tiles, int n_jobs, int n_splits, double* partials,
                         int mode, int flush_every, int* err, cudaStream_t st) {
   if (mode != LEMC_GRAM_BF16X3 && mode != LEMC_GRAM_BF16X4 && mode != LEMC_GRAM_TF32X3)
     return LEMC_ERR_ARG;
-  if (ldv % 64 != 0 || Wpad % 64 != 0 || n_jobs <= 0 || Wpad > ldv) return LEMC_ERR_ARG;
-  if (reinterpret_cast<uintptr_t>(V) % 16 != 0) return LEMC_ERR_ARG;
+  if (ldv % 64 != 0 || ldw % 64 != 0 || Wpad % 64 != 0 || n_jobs <= 0 || Wpad > ldv || Wpad > ldw)
+    return LEMC_ERR_ARG;
+  if (reinterpret_cast<uintptr_t>(V) % 256 != 0 || reinterpret_cast<uintptr_t>(rec_w) % 256 != 0)
+    return LEMC_ERR_ARG;
   const bool tf32 = (mode == LEMC_GRAM_TF32X3);
-  const int KC = tf32 ? 32 : 64;
   TcArgs a;
   a.V = V;
   a.ldv = ldv;
   a.total_rows = total_rows;
   a.rec_w = rec_w;
-  a.W = W;
+  a.ldw = ldw;
   a.tiles = tiles;
   a.partials = partials;
-  a.n_chunks_total = Wpad / KC;
+  a.n_chunks_total = Wpad / (tf32 ? Cfg<true>::KC : Cfg<false>::KC);
   a.n_splits = n_splits;
   // TF32 hi/lo reaches ~1e-6 only with a flush per K-chunk; the BF16 split is
   // limited by its 16-bit representation, so a longer FP32 interval costs nothing
   a.flush_every = flush_every > 0 ? flush_every : (tf32 ? 1 : 4);
   a.passes = (mode == LEMC_GRAM_BF16X4) ? 4 : 3;
   a.err = err;
-  const size_t smem = sizeof(Smem) + 1024;
-  if (tf32) {
-    if (cudaFuncSetAttribute(gram_tc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             int(smem)) != cudaSuccess)
-      return LEMC_ERR_CUDA;
-    gram_tc_kernel<true><<<n_jobs, kThreads, smem, st>>>(a);
-  } else {
-    if (cudaFuncSetAttribute(gram_tc_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             int(smem)) != cudaSuccess)
-      return LEMC_ERR_CUDA;
-    gram_tc_kernel<false><<<n_jobs, kThreads, smem, st>>>(a);
-  }
-  return cudaPeekAtLastError() == cudaSuccess ? LEMC_OK : LEMC_ERR_CUDA;
+  return tf32 ? launch_t<true>(a, n_jobs, st) : launch_t<false>(a, n_jobs, st);
 }
 
-int launch_gram_tc_reduce(const double* partials, const int* tile_of, int n_pi, int n_pj,
-                          int n_tiles, int n_splits, const int32_t* sec_row,
-                          const int32_t* sec_dim, const int32_t* sec_goff, int n_sec,
-                          int max_dim, double* gram, size_t plane, cudaStream_t st) {
+int launch_gram_tc_reduce(const double* partials, const TcTile* tiles, const TcSector* secs,
+                          int n_sec, int n_tiles, int n_splits, int max_dim, double* gram,
+                          size_t plane, cudaStream_t st) {
   dim3 grid((max_dim * max_dim + 255) / 256, n_sec);
-  gram_tc_reduce_kernel<<<grid, 256, 0, st>>>(partials, tile_of, n_pi, n_pj, n_tiles, n_splits,
-                                              sec_row, sec_dim, sec_goff, n_sec, gram, plane);
+  gram_tc_reduce_kernel<<<grid, 256, 0, st>>>(partials, tiles, secs, n_sec, n_tiles, n_splits,
+                                              gram, plane);
   return cudaPeekAtLastError() == cudaSuccess ? LEMC_OK : LEMC_ERR_CUDA;
 }
 
-size_t gram_tc_smem_bytes() { return sizeof(Smem) + 1024; }
+size_t gram_tc_smem_bytes(int mode) {
+  return mode == LEMC_GRAM_TF32X3 ? sizeof(Smem<true>) + 1024 : sizeof(Smem<false>) + 1024;
+}
 
 }  // namespace lemc

@@ -21,7 +21,7 @@ struct SweepArgs {
   const int32_t* guide_pairs;  // [rows][2*kMaxGuideParts] (part, mult)
   const int32_t* guide_npairs; // [rows]
   int* err;                 // device error word (may be null)
-  int W, N, Npad, T2, m, K;  // Npad >= T2 * G, set by sweep_layout()
+  int W, ldw, N, Npad, T2, m, K;  // rec_w row stride ldw; Npad >= T2 * G (sweep_layout)
   float sigma, invR;
   uint32_t seed_lo, seed_hi;
   uint32_t sweep0;
@@ -65,11 +65,11 @@ int launch_init_walkers(float2* pos, int W, int N, float radius, uint32_t seed_l
 int launch_basis(const float2* rec_p, int W, int K, int N, const BasisNode* prog,
                  int n_nodes, float* V, int ldv, double* series, cudaStream_t st);
 
-int launch_gram_simt(const float* V, int ldv, const float* rec_w, int W,
+int launch_gram_simt(const float* V, int ldv, const float* rec_w, int ldw, int W,
                      const GramJob* jobs, int n_jobs, int n_splits, double* out_set0,
                      size_t plane0, double* out_set1, size_t plane1, cudaStream_t st);
 
-int launch_row_accumulate(const float* V, int ldv, const float* rec_w, int W,
+int launch_row_accumulate(const float* V, int ldv, const float* rec_w, int ldw, int W,
                           const int32_t* row_first, int n_rows, int D,
                           const int32_t* row_re, const int32_t* row_im, double* acc,
                           cudaStream_t st);
@@ -81,14 +81,22 @@ struct TcTile {
   int ksplit; // walker split index
   int slot;   // FP64 partial slot index (ksplit * n_tiles + tile)
 };
-int launch_gram_tc_rows(const float* V, int ldv, int total_rows, const float* rec_w, int W,
+// Where a sector's Gram block lives in the tile list: tile index of V rows
+// (r1, r2) = tile0 + ((r1 - a_base) / 128) * n_bpanels + (r2 - b_base) / 32.
+struct TcSector {
+  int row;        // first V row (Re rows; Im rows follow at +dim)
+  int dim;
+  int goff;       // complex offset of the sector's dim x dim block in a Gram plane
+  int tile0;
+  int a_base, b_base, n_bpanels;
+};
+int launch_gram_tc_rows(const float* V, int ldv, int total_rows, const float* rec_w, int ldw,
                         int Wpad, const TcTile* tiles, int n_jobs, int n_splits, double* partials,
                         int mode, int flush_every, int* err, cudaStream_t st);
-int launch_gram_tc_reduce(const double* partials, const int* tile_of, int n_pi, int n_pj,
-                          int n_tiles, int n_splits, const int32_t* sec_row,
-                          const int32_t* sec_dim, const int32_t* sec_goff, int n_sec,
-                          int max_dim, double* gram, size_t plane, cudaStream_t st);
-size_t gram_tc_smem_bytes();
+int launch_gram_tc_reduce(const double* partials, const TcTile* tiles, const TcSector* secs,
+                          int n_sec, int n_tiles, int n_splits, int max_dim, double* gram,
+                          size_t plane, cudaStream_t st);
+size_t gram_tc_smem_bytes(int mode);
 constexpr int kTcSlot = 128 * 96;  // doubles per partial slot
 
 }  // namespace lemc

@@ -268,7 +268,7 @@ sweep_kernel(const SweepArgs a) {
   for (int k = 0; k < kMaxDegree; ++k)
     if (k < K && (k % G) == gl) a.rec_p[(size_t)k * a.W + w] = acc[k];
   if (gl == 0) {
-    const size_t W = a.W;
+    const size_t W = a.ldw;
     a.rec_w[LEMC_W_ONE * W + w] = 1.f;
     a.rec_w[LEMC_W_R2 * W + w] = h2;
     a.rec_w[LEMC_W_R4 * W + w] = h4;
