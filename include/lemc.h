@@ -174,9 +174,10 @@ LEMC_API int lemc_read_gram(lemc_ctx* ctx, int sector_index, double* S, double* 
  *   C[a][b] = sum w1 * (sum_i cos l theta_i) conj(v_a) v_b, a in s1, b in s2. */
 LEMC_API int lemc_read_cross(lemc_ctx* ctx, int sector_a, int sector_b, double* Ccos,
                     double* Csin, double* Cuser);
-/* Reference-estimator row sums (LEMC_GUIDE_ROW), D x D over all selected rows:
- *   fg[a][b] = sum_{w in row a} v_b/v_a, gg[a][b] = sum |v_b/v_a|^2 (real),
- *   fh[a][b] = sum V(z) v_b/v_a with V = omega r^2 + kappa r^4 given here.
+/* Reference-estimator row averages (LEMC_GUIDE_ROW), D x D over all selected
+ * rows, each averaged over the samples of the walkers guided by row a:
+ *   fg[a][b] = <v_b/v_a>, gg[a][b] = <|v_b/v_a|^2> (real),
+ *   fh[a][b] = <V(z) v_b/v_a> with V = omega r^2 + kappa r^4 given here.
  * Replaces results.fg_ff/gg_ff/fHg_ff (modules/edge_montecarlo.h:15-33). */
 LEMC_API int lemc_read_rows(lemc_ctx* ctx, double omega, double kappa, double* fg,
                    double* gg, double* fh, double* n_samples_per_row);

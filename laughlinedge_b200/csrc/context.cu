@@ -832,17 +832,19 @@ int lemc_read_rows(lemc_ctx* c, double omega, double kappa, double* fg, double* 
                             cudaMemcpyDeviceToHost, c->stream));
   LEMC_TRY(lemc_synchronize(c));
   for (int a = 0; a < D; ++a) {
+    const double n = double(c->meas) * (c->row_first[a + 1] - c->row_first[a]);
+    const double inv = n > 0 ? 1.0 / n : 0.0;
     for (int b = 0; b < D; ++b) {
       const double* q = &acc[(size_t(a) * D + b) * kRowAcc];
       const size_t o = size_t(a) * D + b;
-      if (fg) { fg[2 * o] = q[0]; fg[2 * o + 1] = q[1]; }
-      if (gg) gg[o] = q[2];
+      if (fg) { fg[2 * o] = q[0] * inv; fg[2 * o + 1] = q[1] * inv; }
+      if (gg) gg[o] = q[2] * inv;
       if (fh) {
-        fh[2 * o] = omega * q[3] + kappa * q[5];
-        fh[2 * o + 1] = omega * q[4] + kappa * q[6];
+        fh[2 * o] = (omega * q[3] + kappa * q[5]) * inv;
+        fh[2 * o + 1] = (omega * q[4] + kappa * q[6]) * inv;
       }
     }
-    if (n_per_row) n_per_row[a] = double(c->meas) * (c->row_first[a + 1] - c->row_first[a]);
+    if (n_per_row) n_per_row[a] = n;
   }
   return LEMC_OK;
 }

@@ -202,9 +202,11 @@ def tau_int(series, c=5.0):
     return np.array(out)
 
 
-def reference_matrices(fg, gg, fh):
-    """Reference normalisation: X(a,b) = x[a][b] / sqrt(gg[a][b]) then (X + X^H)/2
-    (modules/edge_mc/em_spectrum.cu:331-335, :383-390)."""
+def reference_matrices(fg, gg, fh, n_row):
+    """Reference normalisation of per-row averages: X(a,b) = <x>[a][b] / sqrt(<gg>[a][b])
+    then (X + X^H)/2 (modules/edge_mc/em_spectrum.cu:318-335, :383-390)."""
+    n = np.asarray(n_row, float)[:, None]
+    fg, gg, fh = fg / n, gg / n, fh / n
     M = fg / np.sqrt(gg)
     H = fh / np.sqrt(gg)
     return 0.5 * (M + M.conj().T), 0.5 * (H + H.conj().T)

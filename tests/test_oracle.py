@@ -65,7 +65,7 @@ def test_oracle_harmonic_degeneracy(oracle, mode):
     for r in range(4):
         if mode == "rows":
             res = oracle.run_rows(N, m, 256, 0.3, 7 + r, 200, 400, [dL])
-            M, H = oracle.reference_matrices(res["fg"], res["gg"], res["fh2"])
+            M, H = oracle.reference_matrices(res["fg"], res["gg"], res["fh2"], res["n_row"])
         else:
             rows, S, H2, _ = oracle.run_gram(N, m, 256, 0.3, 7 + r, 200, 400, [dL])
             d = np.sqrt(np.real(np.diag(S)))
