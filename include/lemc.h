@@ -46,6 +46,7 @@ extern "C" {
 #define LEMC_MAX_DEGREE 24      /* largest power-sum degree k (max Delta L)  */
 #define LEMC_MAX_PARTICLES 1024
 #define LEMC_MAX_GUIDE_PARTS 8  /* distinct parts of a guide partition       */
+#define LEMC_MAX_PROBES 8       /* angular probes l of the cos/sin planes      */
 
 /* ---- enumerations ------------------------------------------------------ */
 enum lemc_guide {
@@ -60,13 +61,12 @@ enum lemc_gram_mode {
 };
 /* weight planes recorded per measurement (rows of the record buffer) */
 enum lemc_weight {
-  LEMC_W_ONE = 0,   /* sample weight of the guide (1 for the Laughlin guide)  */
-  LEMC_W_R2 = 1,    /* sum_i |z_i|^2                                           */
-  LEMC_W_R4 = 2,    /* sum_i |z_i|^4                                           */
-  LEMC_W_COS = 3,   /* sum_i cos(l theta_i), l = lemc_config.angular_probe     */
-  LEMC_W_SIN = 4,   /* sum_i sin(l theta_i)                                    */
-  LEMC_W_USER = 5,  /* caller-supplied per-sample potential U(z) (optional)   */
-  LEMC_N_WEIGHTS = 6
+  LEMC_W_ONE = 0,    /* sample weight of the guide (1 for the Laughlin guide)  */
+  LEMC_W_R2 = 1,     /* sum_i |z_i|^2                                           */
+  LEMC_W_R4 = 2,     /* sum_i |z_i|^4                                           */
+  LEMC_W_USER = 3,   /* caller-supplied per-sample potential U(z) (hook)        */
+  LEMC_W_PROBE0 = 4, /* plane 4+2q: sum_i cos(l_q theta_i); 5+2q: sin(l_q theta_i) */
+  LEMC_N_WEIGHTS = LEMC_W_PROBE0 + 2 * LEMC_MAX_PROBES
 };
 
 /* ---- configuration ------------------------------------------------------ */
@@ -82,7 +82,7 @@ typedef struct lemc_config {
   double radius_scale;      /* R of (z/R)^k in p_k; <= 0 selects sqrt(2 m N) */
   double init_radius;       /* walkers start uniform in this disk; <=0: sqrt(2mN) */
   int32_t gram_mode;        /* enum lemc_gram_mode                           */
-  int32_t angular_probe;    /* l of the cos/sin weight planes (0 = off)      */
+  int32_t reserved1;
   int32_t flush_every;      /* tcgen05 path: K-chunks per FP64 flush (0=auto) */
   int32_t profile;          /* 1: time each kernel family with CUDA events   */
 } lemc_config;
@@ -133,6 +133,8 @@ LEMC_API int lemc_partitions(int particles, const int32_t* sectors, int n_sector
  * partitions on the device and the capacity checks.                         */
 LEMC_API int lemc_create(const lemc_config* cfg, lemc_ctx** out);
 LEMC_API int lemc_destroy(lemc_ctx* ctx);
+/* Gaussian step sigma of subsequent sweeps (step tuning). */
+LEMC_API int lemc_set_step(lemc_ctx* ctx, float sigma);
 /* Walker width G in use (after autotuning). */
 LEMC_API int lemc_lanes_per_walker(const lemc_ctx* ctx, int* lanes);
 /* Select the angular-momentum sectors whose basis is sampled. */
@@ -140,6 +142,12 @@ LEMC_API int lemc_set_sectors(lemc_ctx* ctx, const int32_t* sectors, int n_secto
 /* Guide rows for LEMC_GUIDE_ROW: walker w samples |P_{rows[w % n]}|^2 |Psi|^2,
  * rows index the basis of the selected sectors.  NULL selects every row. */
 LEMC_API int lemc_set_guide_rows(lemc_ctx* ctx, const int32_t* rows, int n_rows);
+/* Angular probes l_0..l_{n-1} (n <= LEMC_MAX_PROBES): every measurement records
+ * sum_i cos(l_q theta_i) and sum_i sin(l_q theta_i), and the cross-sector blocks
+ * between sectors whose dL differ by l_q are accumulated with those weights
+ * (edge density Fourier components, reference em_edgeResponse.tpp:136-163,
+ * and the dynamic structure factor, em_dsf.cu:101-117). */
+LEMC_API int lemc_set_probes(lemc_ctx* ctx, const int32_t* l, int n);
 /* Initial walker positions; host_xy == NULL draws them uniformly in the
  * init disk from the Philox stream (replaces particle_positions_initialize,
  * modules/edge_mc/em_markovchain.cu:223-263). */
@@ -149,6 +157,16 @@ LEMC_API int lemc_init_walkers(lemc_ctx* ctx, const float* host_xy);
  * Replaces burnin + hamiltonian_sampler (em_markovchain.cu:266-334,
  * em_spectrum.cu:16-136) and the mcmc_* launches (em_spectrum.cu:139-208). */
 LEMC_API int lemc_run(lemc_ctx* ctx, int n_sweeps, int measure);
+/* Per-step hook for a caller-defined potential U(z): after each measured
+ * sweep the library calls hook(user, xy, u, W, N, stream) with device
+ * pointers to the walker positions (W x N interleaved x,y floats) and to the
+ * LEMC_W_USER weight plane (W floats, to be written with U of each walker) on
+ * the context's stream, before the S/H/cross accumulation of that step.  A
+ * non-zero return aborts the run with that status.  Replaces the device
+ * lambda argument of excitationResponse_compute (em_edgeResponse.tpp:26-194). */
+typedef int (*lemc_step_hook)(void* user, const float* dev_xy, float* dev_user_plane, int W,
+                              int N, void* stream);
+LEMC_API int lemc_run_hooked(lemc_ctx* ctx, int n_sweeps, lemc_step_hook hook, void* user);
 /* Zero every accumulator (samples, Gram matrices, series, acceptance). */
 LEMC_API int lemc_reset_accumulators(lemc_ctx* ctx);
 LEMC_API int lemc_synchronize(lemc_ctx* ctx);
@@ -169,18 +187,25 @@ LEMC_API int lemc_total_dim(const lemc_ctx* ctx, int* dim);
  * Replaces the device->host copy and block averaging of em_spectrum.cu:256-359. */
 LEMC_API int lemc_read_gram(lemc_ctx* ctx, int sector_index, double* S, double* H2,
                    double* H4, double* n_samples);
-/* Cross-sector Gram with the cos/sin(l theta) planes between two selected
- * sectors (used by the dynamic structure factor, em_dsf.cu:18-158):
- *   C[a][b] = sum w1 * (sum_i cos l theta_i) conj(v_a) v_b, a in s1, b in s2. */
-LEMC_API int lemc_read_cross(lemc_ctx* ctx, int sector_a, int sector_b, double* Ccos,
-                    double* Csin, double* Cuser);
+/* Raw cross-sector sums between two different selected sectors (Da x Db):
+ *   Cuser[a][b] = sum w1 U conj(v_a) v_b,
+ *   Ccos[a][b]  = sum w1 (sum_i cos l theta_i) conj(v_a) v_b,
+ *   Csin[a][b]  = sum w1 (sum_i sin l theta_i) conj(v_a) v_b,
+ * l = |dL_b - dL_a|; Ccos/Csin are zero unless l is a probe.  Any output may
+ * be NULL.  Used by the dynamic structure factor (em_dsf.cu:18-158) and the
+ * excitation response (em_edgeResponse.tpp:26-194). */
+LEMC_API int lemc_read_cross(lemc_ctx* ctx, int sector_a, int sector_b, double* Cuser,
+                             double* Ccos, double* Csin);
 /* Reference-estimator row averages (LEMC_GUIDE_ROW), D x D over all selected
  * rows, each averaged over the samples of the walkers guided by row a:
  *   fg[a][b] = <v_b/v_a>, gg[a][b] = <|v_b/v_a|^2> (real),
- *   fh[a][b] = <V(z) v_b/v_a> with V = omega r^2 + kappa r^4 given here.
+ *   fh[a][b] = <V(z) v_b/v_a> with V = omega r^2 + kappa r^4 given here,
+ *   fcos/fsin[a][b] = <sum_i cos/sin(l_0 theta_i) v_b/v_a> (first probe),
+ *   fuser[a][b] = <U(z) v_b/v_a> (hooked runs).  Outputs may be NULL.
  * Replaces results.fg_ff/gg_ff/fHg_ff (modules/edge_montecarlo.h:15-33). */
 LEMC_API int lemc_read_rows(lemc_ctx* ctx, double omega, double kappa, double* fg,
-                   double* gg, double* fh, double* n_samples_per_row);
+                   double* gg, double* fh, double* fcos, double* fsin, double* fuser,
+                   double* n_samples_per_row);
 LEMC_API int lemc_read_stats(lemc_ctx* ctx, lemc_stats* st);
 LEMC_API int lemc_read_positions(lemc_ctx* ctx, float* host_xy);
 /* Walker-mean series of Re/Im p_1..p_4 per measurement: series[m*8 + 2(k-1) + c]. */
@@ -192,12 +217,12 @@ LEMC_API int lemc_read_series(lemc_ctx* ctx, double* series, int max_meas, int* 
  * sweep index sweep0, then (measure != 0) one measurement record.
  *   pos      [W][N] float2, in/out
  *   rec_p    [K][W] float2, p_k for k = 1..K  (out, measure != 0)
- *   rec_w    [LEMC_N_WEIGHTS][W] float        (out, measure != 0)
+ *   rec_w    [4 + 2 n_probes][W] float       (out, measure != 0; USER plane = 0)
  *   accepted [W] uint32, accumulated          (in/out, may be NULL)       */
 LEMC_API int lemc_sweep_device(void* pos, int W, int N, int m, float sigma,
                       uint64_t seed, uint32_t sweep0, int n_sweeps, int K,
                       double radius_scale, int lanes_per_walker, int measure,
-                      int angular_probe, void* rec_p, void* rec_w,
+                      const int32_t* probes, int n_probes, void* rec_p, void* rec_w,
                       void* accepted, void* stream);
 /* Basis build: V[row][w] (float, row stride ldv >= W) for the rows of the
  * selected sectors of ctx, from records rec_p [K][W]. */
@@ -207,6 +232,27 @@ LEMC_API int lemc_basis_device(lemc_ctx* ctx, const void* rec_p, int W, void* V,
  * into the device accumulator of ctx using the given mode. */
 LEMC_API int lemc_gram_device(lemc_ctx* ctx, const void* V, const void* rec_w, int W,
                      int ldv, int gram_mode, void* stream);
+
+/* ---- occupation numbers (two-state walker) -------------------------------
+ * <f_L| a^dagger_l a_l |f_R> for every ordered pair (L, R) of basis rows of
+ * sector dL, l < l_cutoff.  Each walker carries N+1 particles: particle 0
+ * belongs to the bra only, particle N to the ket only, 1..N-1 to both; the
+ * sampled weight is |f_L(z_0..z_{N-1})| |f_R(z_1..z_N)| and the estimator per
+ * sample is sum_l exp(-ln(2 pi l!) + l ln(z_0 conj(z_N) / 2)
+ * - (|z_0|^2 + |z_N|^2)/4 + i phase), phase = arg(P_R/P_L)
+ * + m arg prod_{i=1}^{N-1} (z_i - z_N)/(z_0 - z_i).
+ * out[((L*D + R)*l_cutoff + l)*2 + {0,1}] receives the per-pair averages (not
+ * normalised to N).  Walkers are split into equal contiguous blocks per pair.
+ * Replaces greenFunctionMC::occupation_numbers_sampler and on_compute
+ * (modules/green_function/gf_occupation_numbers.cu:16-239, :309-544). */
+typedef struct lemc_occupation_config {
+  int32_t particles, inverse_filling, dL, l_cutoff;
+  int32_t n_walkers;
+  float step_sigma;
+  uint64_t seed;
+  int32_t burn_in, sweeps;
+} lemc_occupation_config;
+LEMC_API int lemc_occupation(const lemc_occupation_config* cfg, double* out, double* acceptance);
 
 /* ---- FP64 dense tail ----------------------------------------------------
  * Generalized Hermitian eigenproblem H c = E M c (complex D x D, interleaved).

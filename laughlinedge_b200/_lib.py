@@ -21,10 +21,11 @@ STATUS = {0: "ok", -1: "invalid argument", -2: "capacity exceeded", -3: "CUDA er
           -7: "no CUDA device", -8: "file i/o error"}
 
 GUIDE_LAUGHLIN, GUIDE_ROW = 0, 1
+MAX_PROBES = 8
 GRAM_FP64, GRAM_BF16X3, GRAM_BF16X4, GRAM_TF32X3 = 0, 1, 2, 3
 MAX_DEGREE = 24
-N_WEIGHTS = 6
-W_ONE, W_R2, W_R4, W_COS, W_SIN, W_USER = range(6)
+W_ONE, W_R2, W_R4, W_USER, W_PROBE0 = range(5)
+N_WEIGHTS = W_PROBE0 + 2 * MAX_PROBES
 
 
 class LemcError(RuntimeError):
@@ -38,7 +39,7 @@ class Config(C.Structure):
                 ("n_walkers", C.c_int32), ("lanes_per_walker", C.c_int32),
                 ("step_sigma", C.c_float), ("guide", C.c_int32), ("seed", C.c_uint64),
                 ("radius_scale", C.c_double), ("init_radius", C.c_double),
-                ("gram_mode", C.c_int32), ("angular_probe", C.c_int32),
+                ("gram_mode", C.c_int32), ("reserved1", C.c_int32),
                 ("flush_every", C.c_int32), ("profile", C.c_int32)]
 
 
@@ -49,12 +50,19 @@ class Stats(C.Structure):
                 ("ms_basis", C.c_double), ("ms_gram", C.c_double)]
 
 
+class OccConfig(C.Structure):
+    _fields_ = [("particles", C.c_int32), ("inverse_filling", C.c_int32), ("dL", C.c_int32),
+                ("l_cutoff", C.c_int32), ("n_walkers", C.c_int32), ("step_sigma", C.c_float),
+                ("seed", C.c_uint64), ("burn_in", C.c_int32), ("sweeps", C.c_int32)]
+
+
 class PartitionRow(C.Structure):
     _fields_ = [("dL", C.c_int32), ("sector_size", C.c_int32), ("n_pairs", C.c_int32),
                 ("pairs_off", C.c_int32)]
 
 
 PROFILE_FN = C.CFUNCTYPE(C.c_double, C.c_double, C.c_void_p)
+STEP_HOOK = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p)
 
 _P = C.c_void_p
 _I = C.c_int
@@ -83,12 +91,16 @@ _SIGNATURES = {
     "lemc_total_dim": ([_P, _IP], _I),
     "lemc_read_gram": ([_P, _I, _DP, _DP, _DP, _DP], _I),
     "lemc_read_cross": ([_P, _I, _I, _DP, _DP, _DP], _I),
-    "lemc_read_rows": ([_P, _D, _D, _DP, _DP, _DP, _DP], _I),
+    "lemc_read_rows": ([_P, _D, _D, _DP, _DP, _DP, _DP, _DP, _DP, _DP], _I),
+    "lemc_set_step": ([_P, C.c_float], _I),
+    "lemc_occupation": ([C.POINTER(OccConfig), _DP, _DP], _I),
     "lemc_read_stats": ([_P, C.POINTER(Stats)], _I),
     "lemc_read_positions": ([_P, _FP], _I),
     "lemc_read_series": ([_P, _DP, _I, _IP], _I),
     "lemc_sweep_device": ([_P, _I, _I, _I, C.c_float, C.c_uint64, C.c_uint32, _I, _I, _D, _I, _I,
-                           _I, _P, _P, _P, _P], _I),
+                           _I32P, _I, _P, _P, _P, _P], _I),
+    "lemc_set_probes": ([_P, _I32P, _I], _I),
+    "lemc_run_hooked": ([_P, _I, STEP_HOOK, _P], _I),
     "lemc_basis_device": ([_P, _P, _I, _P, _I, _P], _I),
     "lemc_gram_device": ([_P, _P, _P, _I, _I, _I, _P], _I),
     "lemc_geneig": ([_I, _DP, _DP, _D, _DP, _DP, _IP], _I),

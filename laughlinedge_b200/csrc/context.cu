@@ -117,6 +117,7 @@ struct lemc_ctx {
   int n_gram_jobs = 0, n_cross_jobs = 0;
   std::vector<int> row_vre, row_vim;  // V rows of each basis row
 
+  std::vector<int> probes;  // angular probes l_q
   // guide rows
   std::vector<int32_t> walker_row;
   std::vector<int32_t> row_first;  // walkers of row a: [row_first[a], row_first[a+1])
@@ -145,6 +146,7 @@ struct lemc_ctx {
   int tc_splits = 1;
 
   bool walkers_ready = false;
+  bool hooked = false;  // a user-potential hook fills the USER plane
   uint64_t sweeps = 0, meas = 0, sweeps_at_reset = 0;
   std::vector<double> host_series;  // [meas][8]
   double ms_sweep = 0, ms_basis = 0, ms_gram = 0;
@@ -235,6 +237,51 @@ int alloc_records(lemc_ctx* c) {
 
 int setup_tc(lemc_ctx* c);
 
+// SIMT job list: same-sector Gram tiles {ONE, R2, R4} and, for every ordered
+// pair of sectors (diagonal pairs included), cross tiles {USER, COS_l, SIN_l}
+// with l = |dL_j - dL_i| (cos/sin disabled unless l is a probe).
+int build_jobs(lemc_ctx* c) {
+  const auto& sec = c->basis.sectors;
+  std::vector<GramJob> jobs;
+  for (size_t s = 0; s < sec.size(); ++s) {
+    const int dim = c->basis.sector_dim[s];
+    for (int a0 = 0; a0 < dim; a0 += 16)
+      for (int b0 = 0; b0 < dim; b0 += 16)
+        jobs.push_back({c->sec_row[s], dim, c->sec_row[s], dim, a0, b0,
+                        {LEMC_W_ONE, LEMC_W_R2, LEMC_W_R4}, 0, c->sec_goff[s]});
+  }
+  c->n_gram_jobs = int(jobs.size());
+  c->cross_pairs.clear();
+  c->cross_off.clear();
+  size_t coff = 0;
+  for (size_t i = 0; i < sec.size(); ++i)
+    for (size_t j = 0; j < sec.size(); ++j) {
+      const int l = std::abs(sec[j] - sec[i]);
+      int pc = -1, ps = -1;
+      for (size_t q = 0; q < c->probes.size(); ++q)
+        if (c->probes[q] == l) {
+          pc = LEMC_W_PROBE0 + 2 * int(q);
+          ps = pc + 1;
+        }
+      c->cross_pairs.push_back({int(i), int(j)});
+      c->cross_off.push_back(coff);
+      const int da = c->basis.sector_dim[i], db = c->basis.sector_dim[j];
+      for (int a0 = 0; a0 < da; a0 += 16)
+        for (int b0 = 0; b0 < db; b0 += 16)
+          jobs.push_back({c->sec_row[i], da, c->sec_row[j], db, a0, b0, {LEMC_W_USER, pc, ps}, 1,
+                          int(coff)});
+      coff += size_t(da) * db;
+    }
+  c->cross_plane = coff;
+  c->n_cross_jobs = int(jobs.size()) - c->n_gram_jobs;
+  LEMC_TRY(c->jobs.alloc(std::max<size_t>(1, jobs.size())));
+  if (!jobs.empty())
+    LEMC_CUDA(cudaMemcpy(c->jobs.p, jobs.data(), jobs.size() * sizeof(GramJob), cudaMemcpyHostToDevice));
+  LEMC_TRY(c->cross.alloc(6 * std::max<size_t>(1, c->cross_plane)));
+  LEMC_CUDA(cudaMemsetAsync(c->cross.p, 0, sizeof(double) * c->cross.n, c->stream));
+  return LEMC_OK;
+}
+
 int upload_guide(lemc_ctx* c) {
   if (c->cfg.guide != LEMC_GUIDE_ROW || !c->has_basis) return LEMC_OK;
   const int R = int(c->basis.rows.size());
@@ -304,7 +351,8 @@ int sweep_once(lemc_ctx* c, int n_sweeps, int measure) {
   a.n_sweeps = n_sweeps;
   a.measure = measure;
   a.guide = c->cfg.guide;
-  a.angular_probe = c->cfg.angular_probe;
+  a.n_probes = int(c->probes.size());
+  for (int q = 0; q < a.n_probes; ++q) a.probes[q] = c->probes[q];
   return launch_sweep(a, c->G, c->stream);
 }
 
@@ -314,19 +362,20 @@ int gram_step(lemc_ctx* c, const float* V, const float* rec_w, int ldw, int W, i
                                  int(c->basis.rows.size()), c->D, c->d_row_re.p, c->d_row_im.p,
                                  c->rowacc.p, c->stream);
   }
+  const bool cross = c->n_cross_jobs > 0 && (c->hooked || !c->probes.empty());
   if (mode == LEMC_GRAM_FP64) {
     const int splits = std::max(1, std::min(64, W / 1024));
-    return launch_gram_simt(V, c->Wpad, rec_w, ldw, W, c->jobs.p, c->n_gram_jobs + c->n_cross_jobs,
-                            splits, c->gram.p, c->gram_plane, c->cross.p, c->cross_plane,
-                            c->stream);
+    return launch_gram_simt(V, c->Wpad, rec_w, ldw, W, c->jobs.p,
+                            c->n_gram_jobs + (cross ? c->n_cross_jobs : 0), splits, c->gram.p,
+                            c->gram_plane, c->cross.p, c->cross_plane, c->stream);
   }
   if (c->tc_tiles.empty()) LEMC_TRY(setup_tc(c));
   int s = launch_gram_tc_rows(V, c->Wpad, 2 * c->D, rec_w, ldw, c->Wpad, c->d_tc_tiles.p,
                               int(c->tc_tiles.size()), c->tc_splits, c->tc_partials.p, mode,
                               c->cfg.flush_every, c->err.p, c->stream);
   if (s != LEMC_OK) return s;
-  // cross-sector planes (cos/sin/user) are small: FP64 path
-  if (c->n_cross_jobs > 0) {
+  // cross-sector planes (user potential, cos/sin probes): FP64 path
+  if (cross) {
     const int splits = std::max(1, std::min(64, W / 1024));
     s = launch_gram_simt(V, c->Wpad, rec_w, ldw, W, c->jobs.p + c->n_gram_jobs, c->n_cross_jobs,
                          splits, c->gram.p, c->gram_plane, c->cross.p, c->cross_plane, c->stream);
@@ -571,41 +620,8 @@ int lemc_set_sectors(lemc_ctx* c, const int32_t* sectors, int n) {
     }
   }
   c->gram_plane = goff;
-  // cross-sector pairs for the angular probe: dL_b - dL_a == l
-  c->cross_pairs.clear();
-  c->cross_off.clear();
-  size_t coff = 0;
-  if (c->cfg.angular_probe > 0) {
-    for (size_t i = 0; i < sec.size(); ++i)
-      for (size_t j = 0; j < sec.size(); ++j)
-        if (sec[j] - sec[i] == c->cfg.angular_probe) {
-          c->cross_pairs.push_back({int(i), int(j)});
-          c->cross_off.push_back(coff);
-          coff += size_t(c->basis.sector_dim[i]) * c->basis.sector_dim[j];
-        }
-  }
-  c->cross_plane = coff;
-  // SIMT jobs
-  std::vector<GramJob> jobs;
-  for (size_t s = 0; s < sec.size(); ++s) {
-    const int dim = c->basis.sector_dim[s];
-    for (int a0 = 0; a0 < dim; a0 += 16)
-      for (int b0 = 0; b0 < dim; b0 += 16)
-        jobs.push_back({c->sec_row[s], dim, c->sec_row[s], dim, a0, b0, 0, c->sec_goff[s]});
-  }
-  c->n_gram_jobs = int(jobs.size());
-  for (size_t q = 0; q < c->cross_pairs.size(); ++q) {
-    const int i = c->cross_pairs[q].first, j = c->cross_pairs[q].second;
-    const int da = c->basis.sector_dim[i], db = c->basis.sector_dim[j];
-    for (int a0 = 0; a0 < da; a0 += 16)
-      for (int b0 = 0; b0 < db; b0 += 16)
-        jobs.push_back({c->sec_row[i], da, c->sec_row[j], db, a0, b0, 1, int(c->cross_off[q])});
-  }
-  c->n_cross_jobs = int(jobs.size()) - c->n_gram_jobs;
-  LEMC_TRY(c->jobs.alloc(jobs.size()));
-  LEMC_CUDA(cudaMemcpy(c->jobs.p, jobs.data(), jobs.size() * sizeof(GramJob), cudaMemcpyHostToDevice));
+  LEMC_TRY(build_jobs(c));
   LEMC_TRY(c->gram.alloc(6 * c->gram_plane));
-  LEMC_TRY(c->cross.alloc(6 * std::max<size_t>(1, c->cross_plane)));
   LEMC_TRY(build_program(c));
   LEMC_TRY(alloc_records(c));
   c->tc_tiles.clear();
@@ -710,13 +726,39 @@ int lemc_synchronize(lemc_ctx* c) {
   return LEMC_OK;
 }
 
+int lemc_set_step(lemc_ctx* c, float sigma) {
+  if (!c || !(sigma > 0.f)) return LEMC_ERR_ARG;
+  c->cfg.step_sigma = sigma;
+  return LEMC_OK;
+}
+
 int lemc_stream(lemc_ctx* c, void** stream) {
   if (!c || !stream) return LEMC_ERR_ARG;
   *stream = static_cast<void*>(c->stream);
   return LEMC_OK;
 }
 
+static int run_impl(lemc_ctx* c, int n_sweeps, int measure, lemc_step_hook hook, void* user);
+
 int lemc_run(lemc_ctx* c, int n_sweeps, int measure) {
+  return run_impl(c, n_sweeps, measure, nullptr, nullptr);
+}
+
+int lemc_run_hooked(lemc_ctx* c, int n_sweeps, lemc_step_hook hook, void* user) {
+  if (!hook) return LEMC_ERR_ARG;
+  return run_impl(c, n_sweeps, 1, hook, user);
+}
+
+int lemc_set_probes(lemc_ctx* c, const int32_t* l, int n) {
+  if (!c || n < 0 || n > LEMC_MAX_PROBES || (n > 0 && !l)) return LEMC_ERR_ARG;
+  c->probes.assign(l, l + n);
+  for (int q : c->probes)
+    if (q < 0 || q > 1024) return LEMC_ERR_ARG;
+  if (c->has_basis) LEMC_TRY(build_jobs(c));
+  return LEMC_OK;
+}
+
+static int run_impl(lemc_ctx* c, int n_sweeps, int measure, lemc_step_hook hook, void* user) {
   if (!c || n_sweeps < 0) return LEMC_ERR_ARG;
   if (!c->walkers_ready) return LEMC_ERR_STATE;
   if (measure && !c->has_basis) return LEMC_ERR_STATE;
@@ -748,6 +790,13 @@ int lemc_run(lemc_ctx* c, int n_sweeps, int measure) {
     if (c->profile) LEMC_CUDA(cudaEventRecord(c->pev[4 * s + 1], c->stream));
     LEMC_TRY(launch_basis(c->rec_p.p, c->W, c->K, c->N, c->prog.p, c->n_nodes, c->V.p, c->Wpad,
                           c->series.p + 8 * size_t(s), c->stream));
+    if (hook) {
+      c->hooked = true;
+      const int hs = hook(user, reinterpret_cast<const float*>(c->pos.p),
+                          c->rec_w.p + size_t(LEMC_W_USER) * c->Wpad, c->W, c->N,
+                          static_cast<void*>(c->stream));
+      if (hs != LEMC_OK) return hs;
+    }
     if (c->profile) LEMC_CUDA(cudaEventRecord(c->pev[4 * s + 2], c->stream));
     LEMC_TRY(gram_step(c, c->V.p, c->rec_w.p, c->Wpad, c->W, c->cfg.gram_mode));
     if (c->profile) LEMC_CUDA(cudaEventRecord(c->pev[4 * s + 3], c->stream));
@@ -806,13 +855,13 @@ int lemc_read_gram(lemc_ctx* c, int s, double* S, double* H2, double* H4, double
   return LEMC_OK;
 }
 
-int lemc_read_cross(lemc_ctx* c, int sa, int sb, double* Ccos, double* Csin, double* Cuser) {
+int lemc_read_cross(lemc_ctx* c, int sa, int sb, double* Cuser, double* Ccos, double* Csin) {
   if (!c) return LEMC_ERR_ARG;
   if (!c->has_basis) return LEMC_ERR_STATE;
   for (size_t q = 0; q < c->cross_pairs.size(); ++q) {
     if (c->cross_pairs[q].first != sa || c->cross_pairs[q].second != sb) continue;
     const size_t n = size_t(c->basis.sector_dim[sa]) * c->basis.sector_dim[sb];
-    double* outs[3] = {Ccos, Csin, Cuser};
+    double* outs[3] = {Cuser, Ccos, Csin};
     for (int h = 0; h < 3; ++h)
       if (outs[h])
         LEMC_CUDA(cudaMemcpyAsync(outs[h], c->cross.p + 2 * c->cross_plane * h + 2 * c->cross_off[q],
@@ -823,7 +872,7 @@ int lemc_read_cross(lemc_ctx* c, int sa, int sb, double* Ccos, double* Csin, dou
 }
 
 int lemc_read_rows(lemc_ctx* c, double omega, double kappa, double* fg, double* gg, double* fh,
-                   double* n_per_row) {
+                   double* fcos, double* fsin, double* fuser, double* n_per_row) {
   if (!c) return LEMC_ERR_ARG;
   if (!c->has_basis || c->cfg.guide != LEMC_GUIDE_ROW) return LEMC_ERR_STATE;
   const int D = c->D;
@@ -843,6 +892,9 @@ int lemc_read_rows(lemc_ctx* c, double omega, double kappa, double* fg, double* 
         fh[2 * o] = (omega * q[3] + kappa * q[5]) * inv;
         fh[2 * o + 1] = (omega * q[4] + kappa * q[6]) * inv;
       }
+      if (fcos) { fcos[2 * o] = q[7] * inv; fcos[2 * o + 1] = q[8] * inv; }
+      if (fsin) { fsin[2 * o] = q[9] * inv; fsin[2 * o + 1] = q[10] * inv; }
+      if (fuser) { fuser[2 * o] = q[11] * inv; fuser[2 * o + 1] = q[12] * inv; }
     }
     if (n_per_row) n_per_row[a] = n;
   }
@@ -897,8 +949,10 @@ int lemc_read_series(lemc_ctx* c, double* series, int max_meas, int* n_meas) {
 
 int lemc_sweep_device(void* pos, int W, int N, int m, float sigma, uint64_t seed, uint32_t sweep0,
                       int n_sweeps, int K, double radius_scale, int G, int measure,
-                      int angular_probe, void* rec_p, void* rec_w, void* accepted, void* stream) {
+                      const int32_t* probes, int n_probes, void* rec_p, void* rec_w,
+                      void* accepted, void* stream) {
   if (!pos || W <= 0 || N < 2 || m < 1 || K < 1 || K > kMaxDegree) return LEMC_ERR_ARG;
+  if (n_probes < 0 || n_probes > LEMC_MAX_PROBES || (n_probes > 0 && !probes)) return LEMC_ERR_ARG;
   if (measure && (!rec_p || !rec_w)) return LEMC_ERR_ARG;
   if (G <= 0) G = pick_lanes(N);
   if (!sweep_config_ok(G, N)) return LEMC_ERR_CAPACITY;
@@ -921,7 +975,8 @@ int lemc_sweep_device(void* pos, int W, int N, int m, float sigma, uint64_t seed
   a.n_sweeps = n_sweeps;
   a.measure = measure;
   a.guide = LEMC_GUIDE_LAUGHLIN;
-  a.angular_probe = angular_probe;
+  a.n_probes = n_probes;
+  for (int q = 0; q < n_probes; ++q) a.probes[q] = probes[q];
   return launch_sweep(a, G, static_cast<cudaStream_t>(stream));
 }
 

@@ -25,6 +25,7 @@ gram_simt_kernel(const float* __restrict__ V, int ldv, const float* __restrict__
                  int W,
                  const GramJob* __restrict__ jobs, int n_splits, double* __restrict__ out0,
                  size_t plane0, double* __restrict__ out1, size_t plane1) {
+  // plane[h] < 0 disables sum h
   const GramJob jb = jobs[blockIdx.x];
   const int split = blockIdx.y;
   const int per = (W + n_splits - 1) / n_splits;
@@ -37,7 +38,6 @@ gram_simt_kernel(const float* __restrict__ V, int ldv, const float* __restrict__
   const int tx = threadIdx.x % TS, ty = threadIdx.x / TS;
   const int a = jb.a0 + ty, b = jb.b0 + tx;
   double acc[6] = {0, 0, 0, 0, 0, 0};
-  const int p0 = (jb.wset == 0) ? LEMC_W_ONE : LEMC_W_COS;
 
   for (int c0 = wbeg; c0 < wend; c0 += CH) {
     for (int e = threadIdx.x; e < TS * CH; e += blockDim.x) {
@@ -54,12 +54,10 @@ gram_simt_kernel(const float* __restrict__ V, int ldv, const float* __restrict__
       const int h = e / CH, s = e % CH;
       const int wi = c0 + s;
       float v = 0.f;
-      if (wi < wend) {
+      const int pl = jb.plane[h];
+      if (wi < wend && pl >= 0) {
         const float one = rec_w[(size_t)LEMC_W_ONE * ldw + wi];
-        if (jb.wset == 0)
-          v = (h == 0) ? one : one * rec_w[(size_t)(LEMC_W_ONE + h) * ldw + wi];
-        else
-          v = one * rec_w[(size_t)(p0 + h) * ldw + wi];
+        v = (pl == LEMC_W_ONE) ? one : one * rec_w[(size_t)pl * ldw + wi];
       }
       wt[h][s] = v;
     }
@@ -82,8 +80,8 @@ gram_simt_kernel(const float* __restrict__ V, int ldv, const float* __restrict__
   }
   if (a < jb.Da && b < jb.Db) {
     // three weight planes, each `plane` complex entries apart
-    double* out = (jb.wset == 0) ? out0 : out1;
-    const size_t plane = (jb.wset == 0) ? plane0 : plane1;
+    double* out = (jb.buf == 0) ? out0 : out1;
+    const size_t plane = (jb.buf == 0) ? plane0 : plane1;
     if (!out) return;
     const size_t idx = 2 * ((size_t)jb.out + (size_t)a * jb.Db + b);
     atomicAdd(out + idx, acc[0]);
@@ -100,6 +98,7 @@ gram_simt_kernel(const float* __restrict__ V, int ldv, const float* __restrict__
 //   [0,1] sum v_b/v_a      [2] sum |v_b/v_a|^2
 //   [3,4] sum r2 v_b/v_a   [5,6] sum r4 v_b/v_a
 //   [7,8] sum cos v_b/v_a  [9,10] sum sin v_b/v_a   [11,12] sum U v_b/v_a
+// (cos/sin of the first angular probe)
 constexpr int NROWACC = 13;
 
 __global__ void __launch_bounds__(256)
@@ -126,8 +125,8 @@ row_accumulate_kernel(const float* __restrict__ V, int ldv, const float* __restr
       const double one = rec_w[(size_t)LEMC_W_ONE * ldw + w];
       const double h2 = rec_w[(size_t)LEMC_W_R2 * ldw + w];
       const double h4 = rec_w[(size_t)LEMC_W_R4 * ldw + w];
-      const double hc = rec_w[(size_t)LEMC_W_COS * ldw + w];
-      const double hs = rec_w[(size_t)LEMC_W_SIN * ldw + w];
+      const double hc = rec_w[(size_t)LEMC_W_PROBE0 * ldw + w];
+      const double hs = rec_w[(size_t)(LEMC_W_PROBE0 + 1) * ldw + w];
       const double hu = rec_w[(size_t)LEMC_W_USER * ldw + w];
       acc[0] += one * rr;
       acc[1] += one * ri;

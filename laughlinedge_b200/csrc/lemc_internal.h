@@ -28,7 +28,8 @@ struct SweepArgs {
   int n_sweeps;
   int measure;
   int guide;
-  int angular_probe;
+  int n_probes;                  // angular probes l_q recorded as cos/sin planes
+  int probes[LEMC_MAX_PROBES];
 };
 
 // Node of the depth-first basis program: value[depth] = value[depth-1] * p_part
@@ -40,14 +41,18 @@ struct BasisNode {
   int row_im;
 };
 
-// One tile of the SIMT FP64 Gram accumulation.
+// One tile of the SIMT FP64 Gram accumulation: three weighted sums
+//   out_h[a][b] += sum_w ONE(w) * P_h(w) * conj(v_a(w)) v_b(w),
+// P_h = rec_w plane plane[h] (plane[h] == LEMC_W_ONE: no extra factor,
+// plane[h] < 0: the sum is skipped).
 struct GramJob {
   int row_a;   // first V row of the Re part of sector a (Im rows follow at +Da)
   int Da;
   int row_b;
   int Db;
   int a0, b0;  // tile origin inside the (Da x Db) block
-  int wset;    // 0: {ONE, R2, R4}; 1: {COS, SIN, USER}
+  int plane[3];
+  int buf;     // 0: Gram planes, 1: cross planes
   int out;     // offset (in complex entries) of the (Da x Db) block in the output
 };
 

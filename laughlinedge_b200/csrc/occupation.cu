@@ -1,0 +1,337 @@
+// Orbital occupation numbers <f_L| a^dagger_l a_l |f_R> with the two-state
+// walker (reference modules/green_function/green_function.cu:199-373 and
+// gf_occupation_numbers.cu:16-239), all (L, R) pairs of a sector in one launch.
+//
+// A walker carries N+1 particles z_0..z_N: f_L depends on z_0..z_{N-1}, f_R
+// on z_1..z_N, and the walker samples |f_L| |f_R| with
+// f = P_row(z) prod_{i<j} (z_i - z_j)^m exp(-sum |z|^2 / 4).  One sweep moves
+// particle 0, then 1..N-1, then N, each with its own Metropolis test:
+//   0:      |J_0|^m |P_L'/P_L| exp((|z|^2 - |z'|^2)/4)
+//   1..N-1: |c|^m |P_L'/P_L| |P_R'/P_R| |J|^{2m} exp((|z|^2 - |z'|^2)/2),
+//           c = (z'-z_0)(z'-z_N) / ((z-z_0)(z-z_N))
+//   N:      |J_N|^m |P_R'/P_R| exp((|z|^2 - |z'|^2)/4)
+// evaluated as log-ratios.  After every sweep the estimator
+//   sum_l exp(-ln(2 pi l!) + l ln(z_0 conj(z_N)/2) - (|z_0|^2+|z_N|^2)/4 + i phase),
+//   phase = arg(P_R/P_L) + m arg prod_{i=1}^{N-1} (z_i - z_N)/(z_0 - z_i),
+// is accumulated per walker in FP64 (magnitudes by a log-domain recurrence,
+// so nothing under- or overflows for large N), and reduced per pair at the end.
+//
+// One thread per walker; positions in shared memory, interleaved by thread.
+// Random numbers: Philox counter {particle, sweep, walker, 2}, init tag 3.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <vector>
+
+#include "lemc_internal.h"
+#include "lemc_rng.h"
+#include "partitions.hpp"
+
+namespace lemc {
+namespace {
+
+constexpr int kOccThreads = 64;
+constexpr uint32_t kTagOccMove = 2u, kTagOccInit = 3u;
+
+struct OccArgs {
+  int W, N, m, D, Lc;
+  float sigma;
+  float invR;
+  uint32_t k0, k1;
+  int burn, sweeps;
+  const int32_t* pairs;   // [D][2*kMaxGuideParts] (part, mult)
+  const int32_t* npairs;  // [D]
+  double2* acc;           // [Lc][W] per-walker sums
+  uint32_t* accepted;     // [W]
+};
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+__device__ __forceinline__ double2 cpow_d(double2 z, int k) {
+  double2 r = make_double2(1.0, 0.0), b = z;
+  while (k) {
+    if (k & 1) r = cmul(r, b);
+    k >>= 1;
+    if (k) b = cmul(b, b);
+  }
+  return r;
+}
+
+struct Guide {
+  int k[kMaxGuideParts], r[kMaxGuideParts], n;
+  double2 p[kMaxGuideParts];
+};
+
+// log|P'/P| after replacing particle position zo by zn in the guide's power sums
+__device__ __forceinline__ double guide_delta(const Guide& g, float2 zo, float2 zn, float invR,
+                                              double2* pn) {
+  double d = 0.0;
+  const double2 wo = make_double2(zo.x * invR, zo.y * invR), wn = make_double2(zn.x * invR, zn.y * invR);
+  for (int q = 0; q < g.n; ++q) {
+    pn[q] = g.p[q];
+    if (g.k[q] == 0) continue;
+    const double2 a = cpow_d(wo, g.k[q]), b = cpow_d(wn, g.k[q]);
+    pn[q].x += b.x - a.x;
+    pn[q].y += b.y - a.y;
+    d += 0.5 * g.r[q] * (log(pn[q].x * pn[q].x + pn[q].y * pn[q].y) -
+                         log(g.p[q].x * g.p[q].x + g.p[q].y * g.p[q].y));
+  }
+  return d;
+}
+
+__device__ __forceinline__ double guide_arg(const Guide& g) {
+  double a = 0.0;
+  for (int q = 0; q < g.n; ++q)
+    if (g.k[q] > 0) a += g.r[q] * atan2(g.p[q].y, g.p[q].x);
+  return a;
+}
+
+__global__ void __launch_bounds__(kOccThreads) occupation_kernel(const OccArgs a) {
+  extern __shared__ float2 zsm[];
+  const int t = threadIdx.x;
+  const int w = blockIdx.x * kOccThreads + t;
+  const bool live = w < a.W;
+  const int N = a.N, NP = a.N + 1;
+  auto Z = [&](int j) -> float2& { return zsm[j * kOccThreads + t]; };
+
+  const int pair = live ? int((int64_t(w) * a.D * a.D) / a.W) : 0;
+  const int rowL = pair / a.D, rowR = pair % a.D;
+  Guide gl, gr;
+  gl.n = a.npairs[rowL];
+  gr.n = a.npairs[rowR];
+  for (int q = 0; q < kMaxGuideParts; ++q) {
+    gl.k[q] = q < gl.n ? a.pairs[rowL * 2 * kMaxGuideParts + 2 * q] : 0;
+    gl.r[q] = q < gl.n ? a.pairs[rowL * 2 * kMaxGuideParts + 2 * q + 1] : 0;
+    gr.k[q] = q < gr.n ? a.pairs[rowR * 2 * kMaxGuideParts + 2 * q] : 0;
+    gr.r[q] = q < gr.n ? a.pairs[rowR * 2 * kMaxGuideParts + 2 * q + 1] : 0;
+  }
+  // initial positions: uniform in the disk of radius sqrt(2 m N)
+  const float r0 = sqrtf(2.f * a.m * N);
+  for (int j = 0; j < NP; ++j) {
+    const U4 r = philox4x32_10(U4{uint32_t(j), 0u, uint32_t(w), kTagOccInit}, a.k0, a.k1);
+    const float rho = r0 * sqrtf(u01(r.x));
+    float sn, cs;
+    sincospif(2.f * u01(r.y), &sn, &cs);
+    Z(j) = make_float2(rho * cs, rho * sn);
+  }
+  uint32_t nacc = 0;
+  const float sigma = a.sigma;
+  const double mm = double(a.m);
+  for (int s = 0; s < a.burn + a.sweeps; ++s) {
+    // refresh guide power sums: left over 0..N-1, right over 1..N
+    for (int q = 0; q < gl.n; ++q) {
+      gl.p[q] = make_double2(0.0, 0.0);
+      if (gl.k[q] > 0)
+        for (int j = 0; j < N; ++j) {
+          const double2 v = cpow_d(make_double2(Z(j).x * a.invR, Z(j).y * a.invR), gl.k[q]);
+          gl.p[q].x += v.x;
+          gl.p[q].y += v.y;
+        }
+    }
+    for (int q = 0; q < gr.n; ++q) {
+      gr.p[q] = make_double2(0.0, 0.0);
+      if (gr.k[q] > 0)
+        for (int j = 1; j <= N; ++j) {
+          const double2 v = cpow_d(make_double2(Z(j).x * a.invR, Z(j).y * a.invR), gr.k[q]);
+          gr.p[q].x += v.x;
+          gr.p[q].y += v.y;
+        }
+    }
+    for (int i = 0; i < NP; ++i) {
+      const U4 r = philox4x32_10(U4{uint32_t(i), uint32_t(s), uint32_t(w), kTagOccMove}, a.k0, a.k1);
+      const float rad = sqrtf(-2.f * logf(u01(r.x)));
+      float sn, cs;
+      sincospif(2.f * u01(r.y), &sn, &cs);
+      const float2 zo = Z(i);
+      const float2 zn = make_float2(zo.x + sigma * (rad * cs), zo.y + sigma * (rad * sn));
+      // Jastrow log|ratio| over the shared particles 1..N-1
+      double lj = 0.0;
+      for (int j = 1; j < N; ++j) {
+        if (j == i) continue;
+        const float2 zj = Z(j);
+        const float dx = zn.x - zj.x, dy = zn.y - zj.y, ex = zo.x - zj.x, ey = zo.y - zj.y;
+        lj += 0.5 * (log(double(dx * dx + dy * dy)) - log(double(ex * ex + ey * ey)));
+      }
+      const double gz = double(zo.x) * zo.x + double(zo.y) * zo.y - (double(zn.x) * zn.x + double(zn.y) * zn.y);
+      double delta;
+      double2 pl[kMaxGuideParts], pr[kMaxGuideParts];
+      if (i == 0) {
+        delta = mm * lj + guide_delta(gl, zo, zn, a.invR, pl) + 0.25 * gz;
+      } else if (i == N) {
+        delta = mm * lj + guide_delta(gr, zo, zn, a.invR, pr) + 0.25 * gz;
+      } else {
+        const float2 z0 = Z(0), zN = Z(N);
+        const double c0 = 0.5 * (log(double((zn.x - z0.x) * (zn.x - z0.x) + (zn.y - z0.y) * (zn.y - z0.y))) -
+                                 log(double((zo.x - z0.x) * (zo.x - z0.x) + (zo.y - z0.y) * (zo.y - z0.y))));
+        const double cN = 0.5 * (log(double((zn.x - zN.x) * (zn.x - zN.x) + (zn.y - zN.y) * (zn.y - zN.y))) -
+                                 log(double((zo.x - zN.x) * (zo.x - zN.x) + (zo.y - zN.y) * (zo.y - zN.y))));
+        delta = mm * (c0 + cN) + guide_delta(gl, zo, zn, a.invR, pl) +
+                guide_delta(gr, zo, zn, a.invR, pr) + 2.0 * mm * lj + 0.5 * gz;
+      }
+      if (delta >= log(double(u01(r.z)))) {
+        Z(i) = zn;
+        ++nacc;
+        if (i < N)
+          for (int q = 0; q < gl.n; ++q) gl.p[q] = pl[q];
+        if (i > 0)
+          for (int q = 0; q < gr.n; ++q) gr.p[q] = pr[q];
+      }
+    }
+    if (s < a.burn || !live) continue;
+    // estimator
+    const float2 z0 = Z(0), zN = Z(N);
+    double2 u = make_double2(1.0, 0.0);
+    for (int i = 1; i < N; ++i) {
+      const float2 zi = Z(i);
+      const double2 num = make_double2(zi.x - zN.x, zi.y - zN.y);
+      const double2 den = make_double2(z0.x - zi.x, z0.y - zi.y);
+      u = cmul(u, make_double2(num.x * den.x + num.y * den.y, num.y * den.x - num.x * den.y));
+      const double nu = sqrt(u.x * u.x + u.y * u.y);
+      if (nu > 0) {
+        u.x /= nu;
+        u.y /= nu;
+      }
+    }
+    const double phase = guide_arg(gr) - guide_arg(gl) + mm * atan2(u.y, u.x);
+    const double2 q0 = make_double2(0.5 * (double(z0.x) * zN.x + double(z0.y) * zN.y),
+                                    0.5 * (double(z0.y) * zN.x - double(z0.x) * zN.y));  // z0 conj(zN) / 2
+    const double lx = 0.5 * log(q0.x * q0.x + q0.y * q0.y);
+    const double phi = atan2(q0.y, q0.x);
+    const double base = -0.25 * (double(z0.x) * z0.x + double(z0.y) * z0.y + double(zN.x) * zN.x +
+                                 double(zN.y) * zN.y) - log(2.0 * 3.14159265358979323846);
+    double la = base;  // log magnitude of term l (log of 1/(2 pi l!) folded in)
+    for (int l = 0; l < a.Lc; ++l) {
+      if (l > 0) la += lx - log(double(l));
+      if (la > -700.0) {
+        const double mag = exp(la);
+        double sn2, cs2;
+        sincos(l * phi + phase, &sn2, &cs2);
+        double2* p = a.acc + size_t(l) * a.W + w;
+        p->x += mag * cs2;
+        p->y += mag * sn2;
+      }
+    }
+  }
+  if (live) a.accepted[w] = nacc;
+}
+
+__global__ void occupation_reduce(const double2* acc, int W, int D, int Lc, double2* out) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  const int pair = blockIdx.y;
+  if (l >= Lc) return;
+  const int w0 = int((int64_t(pair) * W + (int64_t(D) * D) - 1) / (int64_t(D) * D));
+  const int w1 = int((int64_t(pair + 1) * W + (int64_t(D) * D) - 1) / (int64_t(D) * D));
+  double2 s = make_double2(0.0, 0.0);
+  for (int w = w0; w < w1; ++w) {
+    s.x += acc[size_t(l) * W + w].x;
+    s.y += acc[size_t(l) * W + w].y;
+  }
+  out[size_t(pair) * Lc + l] = s;
+}
+
+}  // namespace
+}  // namespace lemc
+
+using namespace lemc;
+
+extern "C" int lemc_occupation(const lemc_occupation_config* cfg, double* out, double* acceptance) {
+  if (!cfg || !out) return LEMC_ERR_ARG;
+  const int N = cfg->particles, m = cfg->inverse_filling, W = cfg->n_walkers, Lc = cfg->l_cutoff;
+  if (N < 2 || m < 1 || W < 1 || Lc < 1 || cfg->dL < 0 || cfg->dL > kMaxDegree || cfg->sweeps < 1 ||
+      cfg->burn_in < 0 || !(cfg->step_sigma > 0.f))
+    return LEMC_ERR_ARG;
+  const size_t smem = size_t(kOccThreads) * (N + 1) * sizeof(float2);
+  if (smem > 227 * 1024) return LEMC_ERR_CAPACITY;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return LEMC_ERR_NODEVICE;
+  }
+  const Basis B = build_basis(N, {cfg->dL});
+  const int D = int(B.rows.size());
+  if (W < D * D) return LEMC_ERR_ARG;  // at least one walker per pair
+  std::vector<int32_t> pairs(size_t(D) * 2 * kMaxGuideParts, 0), np(D, 0);
+  for (int r = 0; r < D; ++r) {
+    const auto& pr = B.rows[r].pairs;
+    if (int(pr.size()) > kMaxGuideParts) return LEMC_ERR_CAPACITY;
+    np[r] = int(pr.size());
+    for (size_t q = 0; q < pr.size(); ++q) {
+      pairs[size_t(r) * 2 * kMaxGuideParts + 2 * q] = pr[q].part;
+      pairs[size_t(r) * 2 * kMaxGuideParts + 2 * q + 1] = pr[q].part > 0 ? pr[q].mult : 0;
+    }
+  }
+  int32_t *d_pairs = nullptr, *d_np = nullptr;
+  double2 *d_acc = nullptr, *d_out = nullptr;
+  uint32_t* d_accp = nullptr;
+  int st = LEMC_OK;
+  auto ok = [&](cudaError_t e) {
+    if (e != cudaSuccess && st == LEMC_OK) st = LEMC_ERR_CUDA;
+    return st == LEMC_OK;
+  };
+  ok(cudaMalloc(&d_pairs, pairs.size() * 4));
+  ok(cudaMalloc(&d_np, np.size() * 4));
+  ok(cudaMalloc(&d_acc, sizeof(double2) * size_t(Lc) * W));
+  ok(cudaMalloc(&d_out, sizeof(double2) * size_t(D) * D * Lc));
+  ok(cudaMalloc(&d_accp, sizeof(uint32_t) * W));
+  if (st == LEMC_OK) {
+    ok(cudaMemcpy(d_pairs, pairs.data(), pairs.size() * 4, cudaMemcpyHostToDevice));
+    ok(cudaMemcpy(d_np, np.data(), np.size() * 4, cudaMemcpyHostToDevice));
+    ok(cudaMemset(d_acc, 0, sizeof(double2) * size_t(Lc) * W));
+  }
+  if (st == LEMC_OK) {
+    OccArgs a;
+    a.W = W;
+    a.N = N;
+    a.m = m;
+    a.D = D;
+    a.Lc = Lc;
+    a.sigma = cfg->step_sigma;
+    a.invR = float(1.0 / std::sqrt(2.0 * m * N));
+    a.k0 = uint32_t(cfg->seed);
+    a.k1 = uint32_t(cfg->seed >> 32);
+    a.burn = cfg->burn_in;
+    a.sweeps = cfg->sweeps;
+    a.pairs = d_pairs;
+    a.npairs = d_np;
+    a.acc = d_acc;
+    a.accepted = d_accp;
+    if (smem > 48 * 1024)
+      ok(cudaFuncSetAttribute(occupation_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    if (st == LEMC_OK) {
+      occupation_kernel<<<(W + kOccThreads - 1) / kOccThreads, kOccThreads, smem>>>(a);
+      ok(cudaPeekAtLastError());
+      occupation_reduce<<<dim3((Lc + 127) / 128, D * D), 128>>>(d_acc, W, D, Lc, d_out);
+      ok(cudaPeekAtLastError());
+      ok(cudaDeviceSynchronize());
+    }
+  }
+  if (st == LEMC_OK) {
+    std::vector<double2> h(size_t(D) * D * Lc);
+    std::vector<uint32_t> acc(W);
+    ok(cudaMemcpy(h.data(), d_out, sizeof(double2) * h.size(), cudaMemcpyDeviceToHost));
+    ok(cudaMemcpy(acc.data(), d_accp, sizeof(uint32_t) * W, cudaMemcpyDeviceToHost));
+    if (st == LEMC_OK) {
+      double tot = 0;
+      for (uint32_t v : acc) tot += v;
+      if (acceptance)
+        *acceptance = tot / (double(W) * (N + 1) * (cfg->burn_in + cfg->sweeps));
+      for (int pr = 0; pr < D * D; ++pr) {
+        const int w0 = int((int64_t(pr) * W + (int64_t(D) * D) - 1) / (int64_t(D) * D));
+        const int w1 = int((int64_t(pr + 1) * W + (int64_t(D) * D) - 1) / (int64_t(D) * D));
+        const double n = double(w1 - w0) * cfg->sweeps;
+        for (int l = 0; l < Lc; ++l) {
+          out[2 * (size_t(pr) * Lc + l)] = h[size_t(pr) * Lc + l].x / n;
+          out[2 * (size_t(pr) * Lc + l) + 1] = h[size_t(pr) * Lc + l].y / n;
+        }
+      }
+    }
+  }
+  cudaFree(d_pairs);
+  cudaFree(d_np);
+  cudaFree(d_acc);
+  cudaFree(d_out);
+  cudaFree(d_accp);
+  return st;
+}

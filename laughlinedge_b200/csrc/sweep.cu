@@ -228,7 +228,10 @@ sweep_kernel(const SweepArgs a) {
   float2 acc[kMaxDegree];
 #pragma unroll
   for (int k = 0; k < kMaxDegree; ++k) acc[k] = make_float2(0.f, 0.f);
-  float h2 = 0.f, h4 = 0.f, hc = 0.f, hs = 0.f;
+  float h2 = 0.f, h4 = 0.f;
+  float hc[LEMC_MAX_PROBES], hs[LEMC_MAX_PROBES];
+#pragma unroll
+  for (int q = 0; q < LEMC_MAX_PROBES; ++q) hc[q] = hs[q] = 0.f;
   const int K = a.K;
   for (int j = gl; j < N; j += G) {
     const float2 z = zs[j];
@@ -245,11 +248,17 @@ sweep_kernel(const SweepArgs a) {
     const float r2 = fmaf(z.x, z.x, z.y * z.y);
     h2 += r2;
     h4 = fmaf(r2, r2, h4);
-    if (a.angular_probe > 0) {
+    if (a.n_probes > 0) {
       const float rinv = rsqrtf(r2);
-      const float2 u = cpowi(make_float2(z.x * rinv, z.y * rinv), a.angular_probe);
-      hc += u.x;
-      hs += u.y;
+      const float2 u = make_float2(z.x * rinv, z.y * rinv);
+#pragma unroll
+      for (int q = 0; q < LEMC_MAX_PROBES; ++q) {
+        if (q < a.n_probes) {
+          const float2 e = cpowi(u, a.probes[q]);
+          hc[q] += e.x;
+          hs[q] += e.y;
+        }
+      }
     }
   }
 #pragma unroll
@@ -261,8 +270,13 @@ sweep_kernel(const SweepArgs a) {
   }
   h2 = group_sum<G>(h2);
   h4 = group_sum<G>(h4);
-  hc = group_sum<G>(hc);
-  hs = group_sum<G>(hs);
+#pragma unroll
+  for (int q = 0; q < LEMC_MAX_PROBES; ++q) {
+    if (q < a.n_probes) {
+      hc[q] = group_sum<G>(hc[q]);
+      hs[q] = group_sum<G>(hs[q]);
+    }
+  }
   if (!live) return;
 #pragma unroll
   for (int k = 0; k < kMaxDegree; ++k)
@@ -272,9 +286,14 @@ sweep_kernel(const SweepArgs a) {
     a.rec_w[LEMC_W_ONE * W + w] = 1.f;
     a.rec_w[LEMC_W_R2 * W + w] = h2;
     a.rec_w[LEMC_W_R4 * W + w] = h4;
-    a.rec_w[LEMC_W_COS * W + w] = hc;
-    a.rec_w[LEMC_W_SIN * W + w] = hs;
     a.rec_w[LEMC_W_USER * W + w] = 0.f;
+#pragma unroll
+    for (int q = 0; q < LEMC_MAX_PROBES; ++q) {
+      if (q < a.n_probes) {
+        a.rec_w[(LEMC_W_PROBE0 + 2 * q) * W + w] = hc[q];
+        a.rec_w[(LEMC_W_PROBE0 + 2 * q + 1) * W + w] = hs[q];
+      }
+    }
   }
 }
 

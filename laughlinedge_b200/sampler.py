@@ -89,6 +89,20 @@ def evolve(M, H, U, rho, profile, end_time, save_step):
     return times, out.view(np.complex128).reshape(ns, max(L, 1))[:, :L], norms
 
 
+def occupation(particles, inverse_filling, dL, l_cutoff, n_walkers, sweeps, burn_in=200,
+               step_sigma=0.3, seed=42):
+    """Occupation averages for every (L, R) row pair of sector dL: complex [D, D, l_cutoff]."""
+    lib = _lib.load()
+    rows, _, _ = partitions(particles, [dL])
+    D = len(rows)
+    cfg = _lib.OccConfig(particles, inverse_filling, dL, l_cutoff, n_walkers, step_sigma, seed,
+                         burn_in, sweeps)
+    out = np.zeros(2 * D * D * l_cutoff)
+    acc = C.c_double()
+    check(lib.lemc_occupation(C.byref(cfg), dptr(out), C.byref(acc)), "lemc_occupation")
+    return out.view(np.complex128).reshape(D, D, l_cutoff), acc.value
+
+
 @dataclass
 class SamplerConfig:
     particles: int
@@ -101,7 +115,6 @@ class SamplerConfig:
     radius_scale: float = 0.0
     init_radius: float = 0.0
     gram_mode: int = _lib.GRAM_FP64
-    angular_probe: int = 0
     flush_every: int = 0
     profile: bool = False
 
@@ -109,18 +122,21 @@ class SamplerConfig:
         return _lib.Config(self.particles, self.inverse_filling, self.n_walkers,
                            self.lanes_per_walker, self.step_sigma, self.guide, self.seed,
                            self.radius_scale, self.init_radius, self.gram_mode,
-                           self.angular_probe, self.flush_every, 1 if self.profile else 0)
+                           0, self.flush_every, 1 if self.profile else 0)
 
 
 class Sampler:
     """One sampling context on the current CUDA device (wraps lemc_ctx)."""
 
-    def __init__(self, cfg: SamplerConfig, sectors, guide_rows=None):
+    def __init__(self, cfg: SamplerConfig, sectors, guide_rows=None, probes=None):
         self.lib = _lib.load()
         self.cfg = cfg
         self._h = C.c_void_p()
         c = cfg.to_c()
         check(self.lib.lemc_create(C.byref(c), C.byref(self._h)), "lemc_create")
+        if probes:
+            pr = np.ascontiguousarray(probes, dtype=np.int32)
+            check(self.lib.lemc_set_probes(self._h, i32ptr(pr), len(pr)), "lemc_set_probes")
         self.sectors = list(sectors)
         sec = np.ascontiguousarray(self.sectors, dtype=np.int32)
         check(self.lib.lemc_set_sectors(self._h, i32ptr(sec), len(sec)), "lemc_set_sectors")
@@ -157,6 +173,16 @@ class Sampler:
     def run(self, n_sweeps: int, measure: bool = True):
         check(self.lib.lemc_run(self._h, int(n_sweeps), 1 if measure else 0), "lemc_run")
 
+    def run_hooked(self, n_sweeps: int, hook):
+        """Measured sweeps; hook(dev_xy, dev_user_plane, W, N, stream) fills U per walker."""
+        def _cb(user, xy, up, W, N, stream):
+            try:
+                return int(hook(xy, up, W, N, stream) or 0)
+            except Exception:  # surface Python errors as an argument error
+                return -1
+        self._hook = _lib.STEP_HOOK(_cb)
+        check(self.lib.lemc_run_hooked(self._h, int(n_sweeps), self._hook, None), "lemc_run_hooked")
+
     def reset(self):
         check(self.lib.lemc_reset_accumulators(self._h), "lemc_reset_accumulators")
 
@@ -182,17 +208,22 @@ class Sampler:
         return tuple(_cplx(b, D) for b in bufs) + (n.value,)
 
     def cross(self, sa: int, sb: int):
+        """(Cuser, Ccos, Csin) raw cross sums between selected sectors sa != sb."""
         Da, Db = self.dims[sa], self.dims[sb]
         bufs = [np.zeros(2 * Da * Db) for _ in range(3)]
         check(self.lib.lemc_read_cross(self._h, sa, sb, *[dptr(b) for b in bufs]), "lemc_read_cross")
         return tuple(b.view(np.complex128).reshape(Da, Db) for b in bufs)
 
-    def rows(self, omega: float, kappa: float):
+    def rows(self, omega: float, kappa: float, extra: bool = False):
+        """Reference-estimator row averages (fg, gg, fh, n[, fcos, fsin, fuser])."""
         D = self.total_dim
         fg, gg, fh = np.zeros(2 * D * D), np.zeros(D * D), np.zeros(2 * D * D)
+        fc, fs, fu = np.zeros(2 * D * D), np.zeros(2 * D * D), np.zeros(2 * D * D)
         n = np.zeros(D)
-        check(self.lib.lemc_read_rows(self._h, omega, kappa, dptr(fg), dptr(gg), dptr(fh), dptr(n)),
-              "lemc_read_rows")
+        check(self.lib.lemc_read_rows(self._h, omega, kappa, dptr(fg), dptr(gg), dptr(fh), dptr(fc),
+                                      dptr(fs), dptr(fu), dptr(n)), "lemc_read_rows")
+        if extra:
+            return _cplx(fg, D), gg.reshape(D, D), _cplx(fh, D), n, _cplx(fc, D), _cplx(fs, D), _cplx(fu, D)
         return _cplx(fg, D), gg.reshape(D, D), _cplx(fh, D), n
 
     def stats(self) -> _lib.Stats:

@@ -423,3 +423,152 @@ int orc_max_threads(void) {
   return 1;
 #endif
 }
+
+/* ------------------------------------------------------------------------
+ * Occupation numbers with the two-state walker (reference
+ * modules/green_function/green_function.cu:199-373 and
+ * gf_occupation_numbers.cu:16-239): N+1 particles, |f_L(z_0..z_{N-1})| |f_R(z_1..z_N)|,
+ * three move types, estimator sum_l exp(-ln(2 pi l!) + l ln(z_0 conj z_N / 2)
+ * - (|z_0|^2+|z_N|^2)/4 + i phase).  Pair (L, R) = rows L, R of one sector;
+ * out[l] receives the average over W walkers x n_meas sweeps (complex).
+ * Philox counter {particle, sweep, walker, 2}, init {particle, 0, walker, 3}.
+ */
+static double gl_lognorm(const cx* p, const int* k, const int* r, int n) {
+  double s = 0;
+  for (int q = 0; q < n; ++q)
+    if (k[q] > 0) s += 0.5 * r[q] * log(p[q].re * p[q].re + p[q].im * p[q].im);
+  return s;
+}
+
+void orc_occupation(int N, int m, int W, double sigma, uint64_t seed, int n_burn, int n_meas,
+                    const int* gkL, const int* grL, int nL, const int* gkR, const int* grR, int nR,
+                    int Lc, double* out, int nthreads) {
+  const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+  const double invR = 1.0 / sqrt(2.0 * m * N);
+  const int NP = N + 1;
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#endif
+  const int nth =
+#ifdef _OPENMP
+      omp_get_max_threads();
+#else
+      1;
+#endif
+  double* priv = (double*)calloc((size_t)nth * 2 * Lc, sizeof(double));
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 1)
+#endif
+  for (int w = 0; w < W; ++w) {
+    int tid = 0;
+#ifdef _OPENMP
+    tid = omp_get_thread_num();
+#endif
+    double* acc = priv + (size_t)tid * 2 * Lc;
+    float z[2 * 1025];
+    const double r0 = sqrt(2.0 * m * N);
+    for (int j = 0; j < NP; ++j) {
+      uint32_t ctr[4] = {(uint32_t)j, 0u, (uint32_t)w, 3u}, key[2] = {k0, k1}, rr[4];
+      orc_philox(ctr, key, rr);
+      const float rho = (float)(r0 * sqrt(u01(rr[0])));
+      const double ang = 2.0 * M_PI * u01(rr[1]);
+      z[2 * j] = (float)(rho * cos(ang));
+      z[2 * j + 1] = (float)(rho * sin(ang));
+    }
+    cx pL[ORC_MAXGP], pR[ORC_MAXGP], nLp[ORC_MAXGP], nRp[ORC_MAXGP];
+    for (int s = 0; s < n_burn + n_meas; ++s) {
+      for (int q = 0; q < nL; ++q) {
+        pL[q].re = pL[q].im = 0;
+        if (gkL[q] == 0) continue;
+        for (int j = 0; j < N; ++j) {
+          cx v = cpowi((cx){z[2 * j] * invR, z[2 * j + 1] * invR}, gkL[q]);
+          pL[q].re += v.re; pL[q].im += v.im;
+        }
+      }
+      for (int q = 0; q < nR; ++q) {
+        pR[q].re = pR[q].im = 0;
+        if (gkR[q] == 0) continue;
+        for (int j = 1; j <= N; ++j) {
+          cx v = cpowi((cx){z[2 * j] * invR, z[2 * j + 1] * invR}, gkR[q]);
+          pR[q].re += v.re; pR[q].im += v.im;
+        }
+      }
+      for (int i = 0; i < NP; ++i) {
+        uint32_t ctr[4] = {(uint32_t)i, (uint32_t)s, (uint32_t)w, 2u}, key[2] = {k0, k1}, rr[4];
+        orc_philox(ctr, key, rr);
+        const double rad = sqrt(-2.0 * log(u01(rr[0]))), ang = 2.0 * M_PI * u01(rr[1]);
+        const float ox = z[2 * i], oy = z[2 * i + 1];
+        const float nx = (float)(ox + sigma * rad * cos(ang)), ny = (float)(oy + sigma * rad * sin(ang));
+        double lj = 0;
+        for (int j = 1; j < N; ++j) {
+          if (j == i) continue;
+          const double dx = (double)nx - z[2 * j], dy = (double)ny - z[2 * j + 1];
+          const double ex = (double)ox - z[2 * j], ey = (double)oy - z[2 * j + 1];
+          lj += 0.5 * (log(dx * dx + dy * dy) - log(ex * ex + ey * ey));
+        }
+        const double gz = ((double)ox * ox + (double)oy * oy) - ((double)nx * nx + (double)ny * ny);
+        const cx wo = {ox * invR, oy * invR}, wn = {nx * invR, ny * invR};
+        double dlL = 0, dlR = 0;
+        if (i < N) {
+          for (int q = 0; q < nL; ++q) {
+            nLp[q] = pL[q];
+            if (gkL[q] == 0) continue;
+            cx a = cpowi(wo, gkL[q]), b = cpowi(wn, gkL[q]);
+            nLp[q].re += b.re - a.re; nLp[q].im += b.im - a.im;
+          }
+          dlL = gl_lognorm(nLp, gkL, grL, nL) - gl_lognorm(pL, gkL, grL, nL);
+        }
+        if (i > 0) {
+          for (int q = 0; q < nR; ++q) {
+            nRp[q] = pR[q];
+            if (gkR[q] == 0) continue;
+            cx a = cpowi(wo, gkR[q]), b = cpowi(wn, gkR[q]);
+            nRp[q].re += b.re - a.re; nRp[q].im += b.im - a.im;
+          }
+          dlR = gl_lognorm(nRp, gkR, grR, nR) - gl_lognorm(pR, gkR, grR, nR);
+        }
+        double delta;
+        if (i == 0 || i == N) {
+          delta = m * lj + dlL + dlR + 0.25 * gz;
+        } else {
+          const double z0x = z[0], z0y = z[1], zNx = z[2 * N], zNy = z[2 * N + 1];
+          const double c0 = 0.5 * (log((nx - z0x) * (nx - z0x) + (ny - z0y) * (ny - z0y)) -
+                                   log((ox - z0x) * (ox - z0x) + (oy - z0y) * (oy - z0y)));
+          const double cN = 0.5 * (log((nx - zNx) * (nx - zNx) + (ny - zNy) * (ny - zNy)) -
+                                   log((ox - zNx) * (ox - zNx) + (oy - zNy) * (oy - zNy)));
+          delta = m * (c0 + cN) + dlL + dlR + 2.0 * m * lj + 0.5 * gz;
+        }
+        if (delta >= log(u01(rr[2]))) {
+          z[2 * i] = nx; z[2 * i + 1] = ny;
+          if (i < N) for (int q = 0; q < nL; ++q) pL[q] = nLp[q];
+          if (i > 0) for (int q = 0; q < nR; ++q) pR[q] = nRp[q];
+        }
+      }
+      if (s < n_burn) continue;
+      const double z0x = z[0], z0y = z[1], zNx = z[2 * N], zNy = z[2 * N + 1];
+      double ph = 0;
+      for (int q = 0; q < nR; ++q) if (gkR[q] > 0) ph += grR[q] * atan2(pR[q].im, pR[q].re);
+      for (int q = 0; q < nL; ++q) if (gkL[q] > 0) ph -= grL[q] * atan2(pL[q].im, pL[q].re);
+      double jarg = 0;
+      for (int i = 1; i < N; ++i) {
+        jarg += atan2(z[2 * i + 1] - zNy, z[2 * i] - zNx) - atan2(z0y - z[2 * i + 1], z0x - z[2 * i]);
+      }
+      ph += m * jarg;
+      const double qx = 0.5 * (z0x * zNx + z0y * zNy), qy = 0.5 * (z0y * zNx - z0x * zNy);
+      const double lx = 0.5 * log(qx * qx + qy * qy), phi = atan2(qy, qx);
+      double la = -0.25 * (z0x * z0x + z0y * z0y + zNx * zNx + zNy * zNy) - log(2.0 * M_PI);
+      for (int l = 0; l < Lc; ++l) {
+        if (l > 0) la += lx - log((double)l);
+        const double mag = exp(la);
+        acc[2 * l] += mag * cos(l * phi + ph);
+        acc[2 * l + 1] += mag * sin(l * phi + ph);
+      }
+    }
+  }
+  for (int l = 0; l < 2 * Lc; ++l) {
+    double v = 0;
+    for (int t = 0; t < nth; ++t) v += priv[(size_t)t * 2 * Lc + l];
+    out[l] = v / ((double)W * n_meas);
+  }
+  free(priv);
+}

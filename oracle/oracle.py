@@ -210,3 +210,26 @@ def reference_matrices(fg, gg, fh, n_row):
     M = fg / np.sqrt(gg)
     H = fh / np.sqrt(gg)
     return 0.5 * (M + M.conj().T), 0.5 * (H + H.conj().T)
+
+
+def occupation(N, m, W, sigma, seed, n_burn, n_meas, dL, rowL, rowR, Lc, nthreads=0):
+    """Occupation averages of the pair (rowL, rowR) of sector dL: complex [Lc]."""
+    lib = load()
+    rows = partitions(N, [dL])
+
+    def parts(r):
+        pr = rows[r][1]
+        k = np.zeros(MAXGP, np.int32)
+        m_ = np.zeros(MAXGP, np.int32)
+        for q, (kk, mm) in enumerate(pr):
+            k[q] = kk
+            m_[q] = mm if kk > 0 else 0
+        return k, m_, len(pr)
+
+    kL, rL, nL = parts(rowL)
+    kR, rR, nR = parts(rowR)
+    out = np.zeros(2 * Lc)
+    lib.orc_occupation(C.c_int(N), C.c_int(m), C.c_int(W), C.c_double(sigma), C.c_uint64(seed),
+                       C.c_int(n_burn), C.c_int(n_meas), _p(kL), _p(rL), C.c_int(nL), _p(kR),
+                       _p(rR), C.c_int(nR), C.c_int(Lc), _p(out), C.c_int(nthreads))
+    return out.view(np.complex128)

@@ -24,11 +24,14 @@ def dev_sweep(lemc, torch, pos_np, m, sigma, seed, sweep0, n_sweeps, K, R, G, me
     W, N = pos_np.shape[:2]
     pos = torch.from_numpy(np.ascontiguousarray(pos_np, np.float32)).cuda()
     rec_p = torch.zeros((K, W, 2), dtype=torch.float32, device="cuda")
-    rec_w = torch.zeros((6, W), dtype=torch.float32, device="cuda")
+    nprb = 1 if lprobe else 0
+    rec_w = torch.zeros((4 + 2 * nprb, W), dtype=torch.float32, device="cuda")
     acc = torch.zeros(W, dtype=torch.int32, device="cuda")
+    prb = np.array([lprobe], np.int32)
     st = lib.lemc_sweep_device(C.c_void_p(pos.data_ptr()), W, N, m, sigma, seed, sweep0, n_sweeps,
-                               K, R, G, measure, lprobe, C.c_void_p(rec_p.data_ptr()),
-                               C.c_void_p(rec_w.data_ptr()), C.c_void_p(acc.data_ptr()), None)
+                               K, R, G, measure, lemc._lib.i32ptr(prb), nprb,
+                               C.c_void_p(rec_p.data_ptr()), C.c_void_p(rec_w.data_ptr()),
+                               C.c_void_p(acc.data_ptr()), None)
     assert st == 0, st
     torch.cuda.synchronize()
     return (pos.cpu().numpy(), rec_p.cpu().numpy(), rec_w.cpu().numpy(),
@@ -77,9 +80,9 @@ def test_records_match_oracle(lemc, oracle, cuda_ctx):
     assert np.max(np.abs(p_g - p_o) / scale) < 2e-6
     assert np.allclose(rw[1], w_o[:, 1], rtol=2e-6)
     assert np.allclose(rw[2], w_o[:, 2], rtol=2e-6)
-    assert np.allclose(rw[3], w_o[:, 3], atol=2e-5)
-    assert np.allclose(rw[4], w_o[:, 4], atol=2e-5)
-    assert np.all(rw[0] == 1.0)
+    assert np.allclose(rw[4], w_o[:, 3], atol=2e-5)  # cos(3 theta) plane
+    assert np.allclose(rw[5], w_o[:, 4], atol=2e-5)  # sin(3 theta) plane
+    assert np.all(rw[0] == 1.0) and np.all(rw[3] == 0.0)
 
 
 def _sampler(lemc, **kw):
@@ -99,8 +102,8 @@ def test_basis_and_fp64_gram_match_oracle(lemc, oracle, cuda_ctx):
     gpos, rp, rw, _ = dev_sweep(lemc, torch, pos0, m, 0.3, seed, 0, 2, K, R, 8, measure=1)
     Wpad = (W + 63) // 64 * 64
     rec_p = torch.from_numpy(np.ascontiguousarray(rp)).cuda()
-    rec_w = torch.zeros((6, Wpad), dtype=torch.float32, device="cuda")
-    rec_w[:, :W] = torch.from_numpy(rw).cuda()
+    rec_w = torch.zeros((lemc._lib.N_WEIGHTS, Wpad), dtype=torch.float32, device="cuda")
+    rec_w[:rw.shape[0], :W] = torch.from_numpy(rw).cuda()
     D = smp.total_dim
     V = torch.zeros((2 * D, Wpad), dtype=torch.float32, device="cuda")
     assert lib.lemc_basis_device(smp._h, C.c_void_p(rec_p.data_ptr()), W, C.c_void_p(V.data_ptr()),
@@ -215,4 +218,52 @@ def test_gpu_row_guide_matches_oracle_move_by_move(lemc, oracle, cuda_ctx):
     close = np.max(np.abs(gpos - opos), axis=(1, 2)) < 1e-3
     assert np.sum(~close) <= 2
     assert abs(st.acceptance - oacc.sum() / (3 * W * N)) < 0.01
+    smp.close()
+
+
+def test_cross_sector_sums_match_numpy(lemc, oracle, cuda_ctx):
+    """USER / cos / sin planes between sector pairs, FP64 path, same records."""
+    torch = cuda_ctx
+    lib = lemc.load()
+    N, m, W, seed = 8, 3, 256, 19
+    sectors = [0, 2, 4]
+    probes = [0, 2, 4]
+    R = math.sqrt(2 * m * N)
+    smp = lemc.Sampler(lemc.SamplerConfig(N, m, W), sectors, probes=probes)
+    K = 4
+    pos0 = oracle.init_walkers(W, N, R, seed)
+    prb = np.array(probes, np.int32)
+    pos = torch.from_numpy(pos0).cuda()
+    rec_p = torch.zeros((K, W, 2), dtype=torch.float32, device="cuda")
+    Wpad = W
+    rec_w = torch.zeros((lemc._lib.N_WEIGHTS, Wpad), dtype=torch.float32, device="cuda")
+    assert lib.lemc_sweep_device(C.c_void_p(pos.data_ptr()), W, N, m, 0.3, seed, 0, 2, K, R, 8, 1,
+                                 lemc._lib.i32ptr(prb), len(probes), C.c_void_p(rec_p.data_ptr()),
+                                 C.c_void_p(rec_w.data_ptr()), None, None) == 0
+    user = torch.rand(W, device="cuda")
+    rec_w[lemc._lib.W_USER] = user
+    V = torch.zeros((2 * smp.total_dim, Wpad), dtype=torch.float32, device="cuda")
+    assert lib.lemc_basis_device(smp._h, C.c_void_p(rec_p.data_ptr()), W, C.c_void_p(V.data_ptr()),
+                                 Wpad, None) == 0
+    assert lib.lemc_gram_device(smp._h, C.c_void_p(V.data_ptr()), C.c_void_p(rec_w.data_ptr()), W,
+                                Wpad, lemc._lib.GRAM_FP64, None) == 0
+    torch.cuda.synchronize()
+    Vh = V.cpu().numpy().astype(np.float64)
+    rw = rec_w.cpu().numpy().astype(np.float64)
+    firsts = np.cumsum([0] + smp.dims)
+    blocks = []
+    for s, d in enumerate(smp.dims):
+        f = firsts[s]
+        blocks.append(Vh[2 * f:2 * f + d] + 1j * Vh[2 * f + d:2 * f + 2 * d])
+    for i in range(3):
+        for j in range(3):
+            Cu, Cc, Cs = smp.cross(i, j)
+            l = abs(sectors[j] - sectors[i])
+            q = probes.index(l)
+            va, vb = blocks[i], blocks[j]
+            ref_u = (va.conj() * rw[lemc._lib.W_USER]) @ vb.T
+            ref_c = (va.conj() * rw[lemc._lib.W_PROBE0 + 2 * q]) @ vb.T
+            ref_s = (va.conj() * rw[lemc._lib.W_PROBE0 + 2 * q + 1]) @ vb.T
+            for X, Y in ((Cu, ref_u), (Cc, ref_c), (Cs, ref_s)):
+                assert np.max(np.abs(X - Y)) <= 1e-11 * max(1.0, np.max(np.abs(Y)))
     smp.close()

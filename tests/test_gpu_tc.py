@@ -31,7 +31,8 @@ def _gram_both(lemc, torch, N, m, W, sectors, rp, rw, mode, flush=0):
     for md in (lemc._lib.GRAM_FP64, mode):
         smp = lemc.Sampler(lemc.SamplerConfig(N, m, W, flush_every=flush), sectors)
         rec_p = torch.from_numpy(np.ascontiguousarray(rp)).cuda()
-        rec_w = torch.from_numpy(np.ascontiguousarray(rw)).cuda()
+        rec_w = torch.zeros((lemc._lib.N_WEIGHTS, Wpad), dtype=torch.float32, device="cuda")
+        rec_w[:rw.shape[0], :W] = torch.from_numpy(np.ascontiguousarray(rw)).cuda()
         V = torch.zeros((2 * smp.total_dim, Wpad), dtype=torch.float32, device="cuda")
         assert lib.lemc_basis_device(smp._h, C.c_void_p(rec_p.data_ptr()), W,
                                      C.c_void_p(V.data_ptr()), Wpad, None) == 0
