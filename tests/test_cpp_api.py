@@ -70,6 +70,6 @@ def test_drop_in_program_runs(lemc, cuda_ctx, tmp_path):
     M = np.loadtxt(out / "dL=3/Statistics/Metric/0.tsv")
     assert np.allclose(M[M[:, 0] == M[:, 1]][:, 2], 1.0, atol=1e-6)  # normalised diagonal
     occ = np.loadtxt(out / "dL=0/Statistics/OccupationNumbers_not_normalized/0.tsv")
-    assert abs(occ[:, 3].sum() - 8.0) < 1e-6  # sum rule, N = 8
+    assert abs(occ[:, 3].sum() - 8.0) < 1e-4  # sum rule, N = 8 (6-decimal files)
     dyn = np.loadtxt(out / "ExternalExcitation/Statistics/edgeDynamics/dL=0/0.tsv")
     assert dyn.shape[0] == 80 and np.all(np.isfinite(dyn))

@@ -10,8 +10,10 @@ from test_gpu_parity import dev_sweep
 
 pytestmark = pytest.mark.gpu
 
-# relative error of normalised entries |X_tc - X_fp64| / sqrt(S_aa S_bb), stated per mode
-TOL = {1: 2e-5, 2: 2e-6, 3: 2e-6}
+# relative error of normalised entries |X_tc - X_fp64| / sqrt(S_aa S_bb), stated per mode:
+# the BF16 hi/lo split carries 16 significant bits (~1e-5 on heavy-tailed sums, with or
+# without the lo*lo product); TF32 hi/lo with a flush per K-chunk stays below 1e-6.
+TOL = {1: 3e-5, 2: 2e-5, 3: 1.5e-6}
 
 
 def _records(lemc, oracle, torch, N, m, W, sectors, seed, sweeps):
