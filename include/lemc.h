@@ -254,6 +254,36 @@ typedef struct lemc_occupation_config {
 } lemc_occupation_config;
 LEMC_API int lemc_occupation(const lemc_occupation_config* cfg, double* out, double* acceptance);
 
+/* Allocation-free form of lemc_occupation.  It has no counterpart in the
+ * reference: the reference allocates and frees its device buffers inside
+ * every call.  This form is for callers that must not allocate device memory
+ * during the call, for example a process whose device memory is already
+ * owned by a caching allocator (cudaMalloc would fail there), or a loop that
+ * cannot take the device-wide synchronisation of cudaFree.
+ *
+ * Same arguments, kernels, results and status codes as lemc_occupation (the
+ * same seed gives the same output).  All device memory it uses is one fixed
+ * static device array of LEMC_OCC_STATIC_SCRATCH_BYTES per device, holding:
+ *   - the row table;
+ *   - 4*W bytes of acceptance counters;
+ *   - 16*l_cutoff*W bytes of per-walker sums;
+ *   - 16*D*D*l_cutoff bytes of per-pair sums (D = basis size of sector dL).
+ * Each part is rounded up to 256 bytes.  A configuration that needs more
+ * returns LEMC_ERR_CAPACITY before any device work.  The call makes no
+ * cudaMalloc or cudaFree and no allocating library call.
+ *
+ * Set-up: the first call on each device resolves the array's device address
+ * with that device current (cudaGetSymbolAddress), which can load the module
+ * onto the device.  Make that first call before any stream capture.
+ *
+ * Concurrency: every call on one device uses the same array, so calls that
+ * overlap on the same device (from several host threads) race and corrupt
+ * each other's results.  Serialise them.  The call itself is synchronous, as
+ * lemc_occupation is. */
+#define LEMC_OCC_STATIC_SCRATCH_BYTES (64u << 20)
+LEMC_API int lemc_occupation_static(const lemc_occupation_config* cfg, double* out,
+                                    double* acceptance);
+
 /* ---- FP64 dense tail ----------------------------------------------------
  * Generalized Hermitian eigenproblem H c = E M c (complex D x D, interleaved).
  * Eigenvalues ascending; eigenvectors (optional, column j = vector j) are

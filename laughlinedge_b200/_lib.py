@@ -94,6 +94,7 @@ _SIGNATURES = {
     "lemc_read_rows": ([_P, _D, _D, _DP, _DP, _DP, _DP, _DP, _DP, _DP], _I),
     "lemc_set_step": ([_P, C.c_float], _I),
     "lemc_occupation": ([C.POINTER(OccConfig), _DP, _DP], _I),
+    "lemc_occupation_static": ([C.POINTER(OccConfig), _DP, _DP], _I),
     "lemc_read_stats": ([_P, C.POINTER(Stats)], _I),
     "lemc_read_positions": ([_P, _FP], _I),
     "lemc_read_series": ([_P, _DP, _I, _IP], _I),

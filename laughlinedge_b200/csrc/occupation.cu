@@ -21,6 +21,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <mutex>
 #include <vector>
 
 #include "lemc_internal.h"
@@ -333,5 +334,156 @@ extern "C" int lemc_occupation(const lemc_occupation_config* cfg, double* out, d
   cudaFree(d_acc);
   cudaFree(d_out);
   cudaFree(d_accp);
+  return st;
+}
+
+// ---- allocation-free variant ----------------------------------------------
+// lemc_occupation_static runs the same two kernels as lemc_occupation, but all
+// device memory beyond the caller's host buffers comes from one fixed,
+// file-scope device array instead of cudaMalloc: the row table, the per-walker
+// accumulators, the per-pair sums and the acceptance counters.  It is for
+// callers that must not allocate device memory during the call: a process
+// whose device memory is already handed to a caching allocator (so cudaMalloc
+// would fail or fragment it), or a loop that cannot afford the implicit device
+// synchronisation of cudaFree.
+namespace lemc {
+namespace {
+
+constexpr size_t kOccStaticBytes = size_t(LEMC_OCC_STATIC_SCRATCH_BYTES);
+constexpr int kOccStaticDevices = 64;
+
+static __device__ __align__(256) unsigned char g_occ_scratch[kOccStaticBytes];
+
+std::mutex g_occ_scratch_mu;
+void* g_occ_scratch_ptr[kOccStaticDevices] = {};
+
+// Address of g_occ_scratch on the current device, resolved once per device
+// with that device current.
+int occ_scratch_address(void** out) {
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return LEMC_ERR_NODEVICE;
+  }
+  if (dev < 0 || dev >= kOccStaticDevices) return LEMC_ERR_CAPACITY;
+  std::lock_guard<std::mutex> lock(g_occ_scratch_mu);
+  if (!g_occ_scratch_ptr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_occ_scratch);
+    if (e != cudaSuccess || !p) {
+      cudaGetLastError();
+      return LEMC_ERR_CUDA;
+    }
+    g_occ_scratch_ptr[dev] = p;
+  }
+  *out = g_occ_scratch_ptr[dev];
+  return LEMC_OK;
+}
+
+constexpr size_t occ_align256(size_t b) { return (b + 255) & ~size_t(255); }
+
+}  // namespace
+}  // namespace lemc
+
+extern "C" int lemc_occupation_static(const lemc_occupation_config* cfg, double* out,
+                                      double* acceptance) {
+  if (!cfg || !out) return LEMC_ERR_ARG;
+  const int N = cfg->particles, m = cfg->inverse_filling, W = cfg->n_walkers, Lc = cfg->l_cutoff;
+  if (N < 2 || m < 1 || W < 1 || Lc < 1 || cfg->dL < 0 || cfg->dL > kMaxDegree || cfg->sweeps < 1 ||
+      cfg->burn_in < 0 || !(cfg->step_sigma > 0.f))
+    return LEMC_ERR_ARG;
+  const size_t smem = size_t(kOccThreads) * (N + 1) * sizeof(float2);
+  if (smem > 227 * 1024) return LEMC_ERR_CAPACITY;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return LEMC_ERR_NODEVICE;
+  }
+  const Basis B = build_basis(N, {cfg->dL});
+  const int D = int(B.rows.size());
+  if (W < D * D) return LEMC_ERR_ARG;  // at least one walker per pair
+  std::vector<int32_t> table(size_t(D) * 2 * kMaxGuideParts + D, 0);
+  int32_t* pairs = table.data();
+  int32_t* np = table.data() + size_t(D) * 2 * kMaxGuideParts;
+  for (int r = 0; r < D; ++r) {
+    const auto& pr = B.rows[r].pairs;
+    if (int(pr.size()) > kMaxGuideParts) return LEMC_ERR_CAPACITY;
+    np[r] = int(pr.size());
+    for (size_t q = 0; q < pr.size(); ++q) {
+      pairs[size_t(r) * 2 * kMaxGuideParts + 2 * q] = pr[q].part;
+      pairs[size_t(r) * 2 * kMaxGuideParts + 2 * q + 1] = pr[q].part > 0 ? pr[q].mult : 0;
+    }
+  }
+  // scratch layout: [row table][accepted W][acc Lc x W][out D*D x Lc], 256-B aligned parts
+  const size_t b_table = occ_align256(table.size() * sizeof(int32_t));
+  const size_t b_accp = occ_align256(sizeof(uint32_t) * size_t(W));
+  const size_t b_acc = occ_align256(sizeof(double2) * size_t(Lc) * W);
+  const size_t b_out = occ_align256(sizeof(double2) * size_t(D) * D * Lc);
+  if (b_table + b_accp + b_acc + b_out > kOccStaticBytes) return LEMC_ERR_CAPACITY;
+  void* base = nullptr;
+  int st = occ_scratch_address(&base);
+  if (st != LEMC_OK) return st;
+  unsigned char* s = static_cast<unsigned char*>(base);
+  int32_t* d_table = reinterpret_cast<int32_t*>(s);
+  uint32_t* d_accp = reinterpret_cast<uint32_t*>(s + b_table);
+  double2* d_acc = reinterpret_cast<double2*>(s + b_table + b_accp);
+  double2* d_out = reinterpret_cast<double2*>(s + b_table + b_accp + b_acc);
+  auto ok = [&](cudaError_t e) {
+    if (e != cudaSuccess && st == LEMC_OK) st = LEMC_ERR_CUDA;
+    return st == LEMC_OK;
+  };
+  // Only the per-walker accumulators must start at zero: the kernel adds
+  // into them.  The table is copied, and the counters and per-pair sums are
+  // written in full by the kernels.
+  ok(cudaMemcpy(d_table, table.data(), table.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+  ok(cudaMemset(d_acc, 0, sizeof(double2) * size_t(Lc) * W));
+  if (st == LEMC_OK) {
+    OccArgs a;
+    a.W = W;
+    a.N = N;
+    a.m = m;
+    a.D = D;
+    a.Lc = Lc;
+    a.sigma = cfg->step_sigma;
+    a.invR = float(1.0 / std::sqrt(2.0 * m * N));
+    a.k0 = uint32_t(cfg->seed);
+    a.k1 = uint32_t(cfg->seed >> 32);
+    a.burn = cfg->burn_in;
+    a.sweeps = cfg->sweeps;
+    a.pairs = d_table;
+    a.npairs = d_table + size_t(D) * 2 * kMaxGuideParts;
+    a.acc = d_acc;
+    a.accepted = d_accp;
+    if (smem > 48 * 1024)
+      ok(cudaFuncSetAttribute(occupation_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    if (st == LEMC_OK) {
+      occupation_kernel<<<(W + kOccThreads - 1) / kOccThreads, kOccThreads, smem>>>(a);
+      ok(cudaPeekAtLastError());
+      occupation_reduce<<<dim3((Lc + 127) / 128, D * D), 128>>>(d_acc, W, D, Lc, d_out);
+      ok(cudaPeekAtLastError());
+      ok(cudaDeviceSynchronize());
+    }
+  }
+  if (st == LEMC_OK) {
+    std::vector<double2> h(size_t(D) * D * Lc);
+    std::vector<uint32_t> acc(W);
+    ok(cudaMemcpy(h.data(), d_out, sizeof(double2) * h.size(), cudaMemcpyDeviceToHost));
+    ok(cudaMemcpy(acc.data(), d_accp, sizeof(uint32_t) * W, cudaMemcpyDeviceToHost));
+    if (st == LEMC_OK) {
+      double tot = 0;
+      for (uint32_t v : acc) tot += v;
+      if (acceptance)
+        *acceptance = tot / (double(W) * (N + 1) * (cfg->burn_in + cfg->sweeps));
+      for (int pr = 0; pr < D * D; ++pr) {
+        const int w0 = int((int64_t(pr) * W + (int64_t(D) * D) - 1) / (int64_t(D) * D));
+        const int w1 = int((int64_t(pr + 1) * W + (int64_t(D) * D) - 1) / (int64_t(D) * D));
+        const double n = double(w1 - w0) * cfg->sweeps;
+        for (int l = 0; l < Lc; ++l) {
+          out[2 * (size_t(pr) * Lc + l)] = h[size_t(pr) * Lc + l].x / n;
+          out[2 * (size_t(pr) * Lc + l) + 1] = h[size_t(pr) * Lc + l].y / n;
+        }
+      }
+    }
+  }
   return st;
 }
