@@ -393,10 +393,13 @@ int setup_tc(lemc_ctx* c) {
   for (int i = 0; i < ns;) {
     const int r0 = c->sec_row[i], d0 = 2 * c->basis.sector_dim[i];
     if (d0 > 128) {
+      // The real Gram block is symmetric: a tile whose B panel lies wholly
+      // above its A slice (32 (y + 1) <= 128 x) is the transpose of a kept
+      // tile and is skipped; A slice x keeps B panels y >= 4 x.
       const int na = (d0 + 127) / 128, nb = (d0 + 31) / 32;
       const int t0 = int(tiles.size());
       for (int x = 0; x < na; ++x)
-        for (int y = 0; y < nb; ++y) tiles.push_back({r0 + 128 * x, r0 + 32 * y});
+        for (int y = 4 * x; y < nb; ++y) tiles.push_back({r0 + 128 * x, r0 + 32 * y});
       secs[i] = {r0, c->basis.sector_dim[i], c->sec_goff[i], t0, r0, r0, nb};
       ++i;
       continue;

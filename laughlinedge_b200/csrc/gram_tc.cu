@@ -8,26 +8,25 @@
 // recovered from the real products of the [Re; Im] row planes afterwards.
 //
 // Precision: each FP32 operand x is split x = hi + lo with hi = bf16(x),
-// lo = bf16(x - hi) (kind::f16) or hi = x truncated to TF32, lo = x - hi
+// lo = bf16(x - hi) (kind::f16) or hi = tf32_rn(x), lo = tf32_rn(x - hi)
 // (kind::tf32).  hi*hi accumulates in one FP32 tensor-memory accumulator and
 // the correction products hi*lo + lo*hi (+ lo*lo) in a second one, so their
-// FP32 rounding stays 2^-8 (BF16) or 2^-11 (TF32) below the result.  Every
-// `flush_every` K-chunks the epilogue warps add both accumulators into
-// compensated FP32 register sums (Knuth's TwoSum: the rounding error of every
-// addition is carried exactly in a second FP32 word, so the running sum keeps
-// ~48 bits however many flushes it takes; double-buffered TMEM lets the MMAs
-// continue meanwhile).  At the end each job adds sum + compensation, in FP64,
-// to its private slot in global memory.
+// FP32 rounding stays 2^-8 (BF16) or 2^-11 (TF32) below the result.  The
+// tensor core's accumulation truncates (a relative bias of about -4e-8 per
+// MMA step), so every `flush_every` K-chunks the epilogue warps move both
+// accumulators out of tensor memory into FP32 register sums (round-to-nearest;
+// double-buffered TMEM lets the MMAs continue meanwhile).  At the end each
+// job adds its sums, in FP64, to its private slot in global memory.
 //
 // Pipeline (576 threads, one CTA per SM):
 //   warp 17      loader: three tiled TMA loads per K-chunk (A panel 128 x KC,
 //                B panel 32 x KC, weight planes 3 x KC; rows past the end are
 //                zero-filled by the TMA unit) into a ring of raw FP32 stages;
-//   warps 12-15  converters: raw FP32 -> weighted, split hi/lo operands in
+//   warps 8-15   converters: raw FP32 -> weighted, split hi/lo operands in
 //                128-byte-swizzled K-major layout (two operand stages);
 //   warp 16      allocates 512 TMEM columns, one lane issues tcgen05.mma;
-//   warps 0-11   epilogue: TMEM lane quarter = warp % 4, column third =
-//                warp / 4, 32 compensated FP32 accumulators per thread.
+//   warps 0-7    epilogue: TMEM lane quarter = warp % 4, column half =
+//                warp / 4, 48 FP32 accumulators per thread.
 // No load uses cluster multicast; every source is this GPU's own memory.
 // Every mbarrier wait is bounded in time; on expiry the kernel records
 // LEMC_ERR_TIMEOUT in the error word, skips its output and unwinds.
@@ -49,8 +48,11 @@ constexpr int kATileBytes = kM * kOpRowBytes;  // 16 KB
 constexpr int kBTileBytes = kN * kOpRowBytes;  // 12 KB
 constexpr int kOpStageBytes = 2 * kATileBytes + 2 * kBTileBytes;  // hi + lo
 constexpr int kOpStages = 2;
-constexpr int kEpiWarps = 12;
-constexpr int kConvWarp0 = 12;
+constexpr int kEpiWarps = 8;
+constexpr int kConvWarp0 = 8;
+constexpr int kConvWarps = 8;
+constexpr int kConvThreads = kConvWarps * 32;
+constexpr int kEpiCols = kN / (kEpiWarps / 4);  // accumulator columns per epilogue thread
 constexpr int kMmaWarp = 16;
 constexpr int kLoadWarp = 17;
 constexpr int kThreads = 18 * 32;
@@ -198,6 +200,12 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t* r) {
         "=r"(r[14]), "=r"(r[15])
       : "r"(taddr));
 }
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t* r) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+                 "=r"(r[6]), "=r"(r[7])
+               : "r"(taddr));
+}
 __device__ __forceinline__ void tmem_wait_ld() {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
@@ -221,13 +229,21 @@ __device__ __forceinline__ void split_bf16x8(const float* x, uint4& hi, uint4& l
   lo = make_uint4(l[0], l[1], l[2], l[3]);
 }
 
+__device__ __forceinline__ uint32_t to_tf32_rn(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
+}
+
+// hi = x rounded to nearest TF32, lo = (x - hi) rounded to nearest TF32: both
+// roundings are unbiased (the tensor core would otherwise truncate the low 13
+// bits of each operand, a systematic -2^-22 relative bias on every product).
 __device__ __forceinline__ void split_tf32x4(const float* x, uint4& hi, uint4& lo) {
   uint32_t h[4], l[4];
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
-    const uint32_t hb = __float_as_uint(x[q]) & 0xFFFFE000u;
-    h[q] = hb;
-    l[q] = __float_as_uint(x[q] - __uint_as_float(hb));
+    h[q] = to_tf32_rn(x[q]);
+    l[q] = to_tf32_rn(x[q] - __uint_as_float(h[q]));
   }
   hi = make_uint4(h[0], h[1], h[2], h[3]);
   lo = make_uint4(l[0], l[1], l[2], l[3]);
@@ -276,10 +292,10 @@ gram_tc_kernel(const TcArgs a, const __grid_constant__ CUtensorMap tmA,
   if (threadIdx.x == 0) {
     for (int s = 0; s < RS; ++s) {
       mbar_init(&sm->raw_full[s], 1);
-      mbar_init(&sm->raw_empty[s], 128);
+      mbar_init(&sm->raw_empty[s], kConvThreads);
     }
     for (int s = 0; s < kOpStages; ++s) {
-      mbar_init(&sm->op_full[s], 128);
+      mbar_init(&sm->op_full[s], kConvThreads);
       mbar_init(&sm->op_empty[s], 1);
     }
     for (int b = 0; b < 2; ++b) {
@@ -318,7 +334,7 @@ gram_tc_kernel(const TcArgs a, const __grid_constant__ CUtensorMap tmA,
       }
     }
     __syncwarp();
-  } else if (warp >= kConvWarp0 && warp < kConvWarp0 + 4) {
+  } else if (warp >= kConvWarp0 && warp < kConvWarp0 + kConvWarps) {
     // ------------------------------ converters -----------------------------
     const int t = threadIdx.x - kConvWarp0 * 32;
     for (int c = 0; c < nch; ++c) {
@@ -334,8 +350,8 @@ gram_tc_kernel(const TcArgs a, const __grid_constant__ CUtensorMap tmA,
       uint8_t* b_lo = b_hi + kBTileBytes;
       // A: 128 rows x 8 operand chunks, unweighted
 #pragma unroll 2
-      for (int q = 0; q < 8; ++q) {
-        const int id = q * 128 + t;
+      for (int q = 0; q < (kM * 8) / kConvThreads; ++q) {
+        const int id = q * kConvThreads + t;
         const int r = id >> 3, ch = id & 7;
         float x[EPC];
         if (tile.row0 + r < a.total_rows) {
@@ -357,8 +373,8 @@ gram_tc_kernel(const TcArgs a, const __grid_constant__ CUtensorMap tmA,
       }
       // B: 32 rows x 8 operand chunks x 3 weight planes
 #pragma unroll 1
-      for (int q = 0; q < 2; ++q) {
-        const int id = q * 128 + t;
+      for (int q = 0; q < (kNB * 8) / kConvThreads; ++q) {
+        const int id = q * kConvThreads + t;
         const int r = id >> 3, ch = id & 7;
         float x[EPC];
         if (tile.col0 + r < a.total_rows) {
@@ -441,45 +457,41 @@ gram_tc_kernel(const TcArgs a, const __grid_constant__ CUtensorMap tmA,
   } else if (warp < kEpiWarps) {
     // ------------------------------- epilogue ------------------------------
     const int quarter = warp & 3;
-    const int third = warp >> 2;
-    float sum[32], cmp[32];
+    const int part0 = (warp >> 2) * kEpiCols;  // first accumulator column of this thread
+    // Plain FP32 running sums (round-to-nearest, unbiased): over n flushes the
+    // relative rounding error is ~2^-24 sqrt(n) / 3 per split, and the FP64
+    // sum over splits averages it down further.  The flushed values are read
+    // eight columns at a time to stay within the register budget.
+    float sum[kEpiCols];
 #pragma unroll
-    for (int i = 0; i < 32; ++i) {
-      sum[i] = 0.f;
-      cmp[i] = 0.f;
-    }
+    for (int i = 0; i < kEpiCols; ++i) sum[i] = 0.f;
     const uint32_t lane_base = uint32_t(quarter * 32) << 16;
     for (int q = 0; q < nint; ++q) {
       const int b = q & 1;
       if (!mbar_wait(&sm->acc_full[b], uint32_t(q >> 1) & 1u, abort_flag, a.err)) break;
       tc_fence_after();
-      const uint32_t ta = tmem + lane_base + uint32_t(b * kBufCols + third * 32);
+      const uint32_t ta = tmem + lane_base + uint32_t(b * kBufCols + part0);
 #pragma unroll
-      for (int half = 0; half < 2; ++half) {
-        uint32_t hv[16], cv[16];
-        tmem_ld16(ta + half * 16, hv);
-        tmem_ld16(ta + 128 + half * 16, cv);
+      for (int part = 0; part < kEpiCols / 8; ++part) {
+        uint32_t hv[8], cv[8];
+        tmem_ld8(ta + part * 8, hv);
+        tmem_ld8(ta + 128 + part * 8, cv);
         tmem_wait_ld();
-#pragma unroll
-        for (int i = 0; i < 16; ++i) {
-          const int k = half * 16 + i;
-          const float y = __uint_as_float(hv[i]) + __uint_as_float(cv[i]);
-          // TwoSum: t + e == sum + y exactly
-          const float t = sum[k] + y;
-          const float z = t - sum[k];
-          const float e = (sum[k] - (t - z)) + (y - z);
-          sum[k] = t;
-          cmp[k] += e;
+        if (part == kEpiCols / 8 - 1) {
+          // every column of this buffer is in registers: the MMAs may reuse it
+          tc_fence_before();
+          mbar_arrive(&sm->acc_empty[b]);
         }
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+          sum[part * 8 + i] += __uint_as_float(hv[i]) + __uint_as_float(cv[i]);
       }
-      tc_fence_before();
-      mbar_arrive(&sm->acc_empty[b]);
     }
     if (!*(volatile int*)abort_flag && nint > 0) {
       double* slot = a.partials + (size_t)tile.slot * (kM * kN) +
-                     (size_t)(quarter * 32 + lane) * kN + third * 32;
+                     (size_t)(quarter * 32 + lane) * kN + part0;
 #pragma unroll
-      for (int i = 0; i < 32; ++i) slot[i] += double(sum[i]) + double(cmp[i]);
+      for (int i = 0; i < kEpiCols; ++i) slot[i] += double(sum[i]);
     }
   }
 
@@ -494,9 +506,10 @@ gram_tc_kernel(const TcArgs a, const __grid_constant__ CUtensorMap tmA,
 // Fold the partial slots into the per-sector complex Gram planes:
 //   G_h[a][b] += sum_splits [C(re a, re b) + C(im a, im b)]
 //              + i [C(re a, im b) - C(im a, re b)]
-// with C(r1, r2) read from the tile that covers A row r1 and B row r2.  Each
+// with C(r1, r2) read from the tile that covers A row r1 and B row r2, or
+// from the tile of C(r2, r1) when that one was skipped by symmetry.  Each
 // sector knows its tiles: first tile index, A/B row origins and the number
-// of B panels (TcSector).
+// of B panels (TcSector); A slice x of a sector holds B panels 4x .. nb-1.
 __global__ void gram_tc_reduce_kernel(const double* __restrict__ partials,
                                       const TcTile* __restrict__ tiles,
                                       const TcSector* __restrict__ secs, int n_sec, int n_tiles,
@@ -509,7 +522,14 @@ __global__ void gram_tc_reduce_kernel(const double* __restrict__ partials,
   if (idx >= D * D) return;
   const int a = idx / D, b = idx % D;
   auto C = [&](int r1, int r2, int h) {
-    const int t = sc.tile0 + ((r1 - sc.a_base) / kM) * sc.n_bpanels + (r2 - sc.b_base) / kNB;
+    // A slice x holds B panels y >= 4 x only (the others are transposes)
+    if ((r2 - sc.b_base) / kNB < 4 * ((r1 - sc.a_base) / kM)) {
+      const int r = r1;
+      r1 = r2;
+      r2 = r;
+    }
+    const int x = (r1 - sc.a_base) / kM, y = (r2 - sc.b_base) / kNB;
+    const int t = sc.tile0 + x * sc.n_bpanels - 2 * x * (x - 1) + (y - 4 * x);
     double v = 0.0;
     if (t < 0 || t >= n_tiles) return v;
     const TcTile tl = tiles[t];
@@ -603,9 +623,11 @@ int launch_gram_tc_rows(const float* V, int ldv, int total_rows, const float* re
   a.partials = partials;
   a.n_chunks_total = Wpad / (tf32 ? Cfg<true>::KC : Cfg<false>::KC);
   a.n_splits = n_splits;
-  // TF32 hi/lo reaches ~1e-6 only with a flush per K-chunk; the BF16 split is
-  // limited by its 16-bit representation, so a longer FP32 interval costs nothing
-  a.flush_every = flush_every > 0 ? flush_every : (tf32 ? 1 : 4);
+  // The tensor core's FP32 accumulation truncates: the relative bias grows by
+  // ~4e-8 per MMA step into one accumulator, so TF32 hi/lo flushes every two
+  // K-chunks (8 steps); the BF16 split is limited by its 16-bit representation,
+  // so a longer interval costs nothing there
+  a.flush_every = flush_every > 0 ? flush_every : (tf32 ? 2 : 4);
   a.passes = (mode == LEMC_GRAM_BF16X4) ? 4 : 3;
   a.err = err;
   return tf32 ? launch_t<true>(a, n_jobs, st) : launch_t<false>(a, n_jobs, st);

@@ -86,8 +86,10 @@ struct TcTile {
   int ksplit; // walker split index
   int slot;   // FP64 partial slot index (ksplit * n_tiles + tile)
 };
-// Where a sector's Gram block lives in the tile list: tile index of V rows
-// (r1, r2) = tile0 + ((r1 - a_base) / 128) * n_bpanels + (r2 - b_base) / 32.
+// Where a sector's Gram block lives in the tile list.  A slice x = (r1 -
+// a_base) / 128 keeps B panels y = (r2 - b_base) / 32 >= 4 x only (the rest
+// are transposes of kept tiles), so the tile of rows (r1, r2) with y >= 4 x is
+// tile0 + x * n_bpanels - 2 x (x - 1) + (y - 4 x).
 struct TcSector {
   int row;        // first V row (Re rows; Im rows follow at +dim)
   int dim;
