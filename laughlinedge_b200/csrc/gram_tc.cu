@@ -10,23 +10,35 @@
 // Precision: each FP32 operand x is split x = hi + lo with hi = bf16(x),
 // lo = bf16(x - hi) (kind::f16) or hi = tf32_rn(x), lo = tf32_rn(x - hi)
 // (kind::tf32).  hi*hi accumulates in one FP32 tensor-memory accumulator and
-// the correction products hi*lo + lo*hi (+ lo*lo) in a second one, so their
-// FP32 rounding stays 2^-8 (BF16) or 2^-11 (TF32) below the result.  The
+// the correction products hi*lo + lo*hi (+ lo*lo) in a second one.  The
 // tensor core's accumulation truncates (a relative bias of about -4e-8 per
-// MMA step), so every `flush_every` K-chunks the epilogue warps move both
-// accumulators out of tensor memory into FP32 register sums (round-to-nearest;
-// double-buffered TMEM lets the MMAs continue meanwhile).  At the end each
-// job adds its sums, in FP64, to its private slot in global memory.
+// MMA step), so every `flush_every` K-chunks the epilogue warps move the hi*hi
+// accumulator out of tensor memory into FP32 register sums (round-to-nearest;
+// two hi*hi buffers let the MMAs continue meanwhile).  The correction
+// accumulator is 2^-11 (TF32) or 2^-8 (BF16) of the result, so its own bias
+// stays far below the target and it is read once, after the last K-chunk.  At
+// the end each job adds its sums, in FP64, to its private slot in global
+// memory.
+//
+// Operand placement.  The A operand (hi and lo, 128 rows x one K-chunk) lives
+// in tensor memory: the A converters write it with tcgen05.st and the MMAs
+// read it from there, so shared memory only carries the raw TMA stages and
+// the (weighted, split) B operand.
 //
 // Pipeline (576 threads, one CTA per SM):
-//   warp 17      loader: three tiled TMA loads per K-chunk (A panel 128 x KC,
-//                B panel 32 x KC, weight planes 3 x KC; rows past the end are
-//                zero-filled by the TMA unit) into a ring of raw FP32 stages;
-//   warps 8-15   converters: raw FP32 -> weighted, split hi/lo operands in
-//                128-byte-swizzled K-major layout (two operand stages);
+//   warp 17      loader: tiled TMA loads per K-chunk (A panel 128 x KC in
+//                128-byte-swizzled boxes of 32 samples, B panel 32 x KC,
+//                weight planes 3 x KC; rows past the end are zero-filled by
+//                the TMA unit) into a ring of raw FP32 stages;
+//   warps 8-11   A converters: thread = A row (TMEM lane); raw FP32 -> hi/lo,
+//                stored to the tensor-memory A stage with tcgen05.st;
+//   warps 12-15  B converters: raw FP32 -> weighted, split hi/lo B operands in
+//                128-byte-swizzled K-major shared-memory layout;
 //   warp 16      allocates 512 TMEM columns, one lane issues tcgen05.mma;
 //   warps 0-7    epilogue: TMEM lane quarter = warp % 4, column half =
 //                warp / 4, 48 FP32 accumulators per thread.
+// Tensor memory columns: hi*hi buffers at 0 and 128, corrections at 256, A
+// stages at 384 and 448 (hi at +0, lo at +32).
 // No load uses cluster multicast; every source is this GPU's own memory.
 // Every mbarrier wait is bounded in time; on expiry the kernel records
 // LEMC_ERR_TIMEOUT in the error word, skips its output and unwinds.
@@ -44,41 +56,45 @@ constexpr int kM = 128;            // A panel rows (MMA M)
 constexpr int kNB = 32;            // B panel rows per weight
 constexpr int kN = 3 * kNB;        // MMA N
 constexpr int kOpRowBytes = 128;   // one swizzle-128B row of split operands
-constexpr int kATileBytes = kM * kOpRowBytes;  // 16 KB
 constexpr int kBTileBytes = kN * kOpRowBytes;  // 12 KB
-constexpr int kOpStageBytes = 2 * kATileBytes + 2 * kBTileBytes;  // hi + lo
 constexpr int kOpStages = 2;
 constexpr int kEpiWarps = 8;
-constexpr int kConvWarp0 = 8;
-constexpr int kConvWarps = 8;
-constexpr int kConvThreads = kConvWarps * 32;
+constexpr int kAConvWarp0 = 8;     // warps 8-11: A converters (lane quarter = warp % 4)
+constexpr int kBConvWarp0 = 12;    // warps 12-15: B converters
+constexpr int kConvThreads = 8 * 32;
 constexpr int kEpiCols = kN / (kEpiWarps / 4);  // accumulator columns per epilogue thread
 constexpr int kMmaWarp = 16;
 constexpr int kLoadWarp = 17;
 constexpr int kThreads = 18 * 32;
-constexpr int kTmemCols = 512;     // 2 buffers x (hi*hi at +0, corrections at +128)
-constexpr int kBufCols = 256;
+constexpr int kTmemCols = 512;
+constexpr uint32_t kColHH = 0;     // hi*hi buffers at 0 and 128
+constexpr uint32_t kColCorr = 256; // corrections
+constexpr uint32_t kColA = 384;    // A stages at 384 + 64 s (hi +0, lo +32)
 constexpr long long kWaitCycles = 4000000000LL;  // ~2 s at 1.9 GHz
 
 template <bool TF32>
 struct Cfg {
   static constexpr int KC = TF32 ? 32 : 64;           // samples per K-chunk
   static constexpr int RAW_ROW = KC * 4;              // bytes of one raw FP32 row segment
-  static constexpr int RAW_W = 3 * KC * 4;            // weight planes of one chunk
-  static constexpr int RAW_STAGE = (kM + kNB) * RAW_ROW + RAW_W;
-  static constexpr int RAW_STAGES = TF32 ? 4 : 2;
+  static constexpr int A_BOXES = KC / 32;             // 128-byte-wide swizzled A boxes
+  static constexpr int A_BYTES = kM * RAW_ROW;        // raw A (all boxes)
+  static constexpr int B_BYTES = kNB * RAW_ROW;
+  static constexpr int W_BYTES = 3 * KC * 4;
+  static constexpr int RAW_STAGE = A_BYTES + B_BYTES + 1024;  // weights padded to 1 KB
+  static constexpr int RAW_STAGES = TF32 ? 6 : 3;
 };
 
 template <bool TF32>
 struct Smem {
-  uint8_t op[kOpStages][kOpStageBytes];  // 1024-aligned operand stages
-  uint8_t raw[Cfg<TF32>::RAW_STAGES][Cfg<TF32>::RAW_STAGE];
+  uint8_t raw[Cfg<TF32>::RAW_STAGES][Cfg<TF32>::RAW_STAGE];  // 1024-aligned stages
+  uint8_t bop[kOpStages][2 * kBTileBytes];                    // B hi | B lo
   uint64_t raw_full[Cfg<TF32>::RAW_STAGES];
   uint64_t raw_empty[Cfg<TF32>::RAW_STAGES];
   uint64_t op_full[kOpStages];
   uint64_t op_empty[kOpStages];
   uint64_t acc_full[2];
   uint64_t acc_empty[2];
+  uint64_t corr_full;
   uint64_t done;
   uint32_t tmem_base;
   int abort_flag;
@@ -157,22 +173,37 @@ __host__ __device__ constexpr uint32_t make_idesc(uint32_t ab_format) {
          (uint32_t(kM >> 4) << 24);
 }
 
+// D (TMEM) += A (TMEM, 128 lanes x K) * B (shared memory descriptor)
 template <bool TF32>
-__device__ __forceinline__ void mma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
-                                    uint32_t accumulate) {
+__device__ __forceinline__ void mma_ts(uint32_t tmem_d, uint32_t tmem_a, uint64_t bdesc,
+                                       uint32_t idesc, uint32_t accumulate) {
   if (TF32) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
-        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "r"(tmem_a), "l"(bdesc), "r"(idesc), "r"(accumulate));
   } else {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
-        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "r"(tmem_a), "l"(bdesc), "r"(idesc), "r"(accumulate));
   }
+}
+
+// 16 consecutive 32-bit columns of this thread's TMEM lane
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t* r) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], "
+      "{%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(taddr),
+      "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]),
+      "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]),
+      "r"(r[15])
+      : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() {
+  asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
 }
 
 __device__ __forceinline__ void umma_commit(uint64_t* bar) {
@@ -191,15 +222,6 @@ __device__ __forceinline__ void fence_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t* r) {
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
-      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-        "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr));
-}
 __device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t* r) {
   asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
@@ -270,7 +292,7 @@ gram_tc_kernel(const TcArgs a, const __grid_constant__ CUtensorMap tmA,
                const __grid_constant__ CUtensorMap tmB, const __grid_constant__ CUtensorMap tmW) {
   using C = Cfg<TF32>;
   constexpr int KC = C::KC;
-  constexpr int EPC = TF32 ? 4 : 8;          // elements per 16-byte operand chunk
+  constexpr int EPC = TF32 ? 4 : 8;          // elements per 16-byte B operand chunk
   constexpr int NKSTEP = kOpRowBytes / 32;   // one MMA consumes 32 bytes of K
   constexpr uint32_t IDESC = make_idesc(TF32 ? 2u : 1u);
   constexpr int RS = C::RAW_STAGES;
@@ -302,6 +324,7 @@ gram_tc_kernel(const TcArgs a, const __grid_constant__ CUtensorMap tmA,
       mbar_init(&sm->acc_full[b], 1);
       mbar_init(&sm->acc_empty[b], kEpiWarps * 32);
     }
+    mbar_init(&sm->corr_full, 1);
     mbar_init(&sm->done, 1);
     sm->abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -321,72 +344,97 @@ gram_tc_kernel(const TcArgs a, const __grid_constant__ CUtensorMap tmA,
   if (warp == kLoadWarp) {
     // ------------------------------- loader --------------------------------
     if (lane == 0) {
-      const uint32_t tx_bytes = uint32_t(C::RAW_STAGE);
+      const uint32_t tx_bytes = uint32_t(C::A_BYTES + C::B_BYTES + C::W_BYTES);
       for (int c = 0; c < nch; ++c) {
         const int s = c % RS;
         if (!mbar_wait(&sm->raw_empty[s], (uint32_t(c / RS) & 1u) ^ 1u, abort_flag, a.err)) break;
         const int k0 = (c_beg + c) * KC;
         uint8_t* dst = sm->raw[s];
         mbar_arrive_tx(&sm->raw_full[s], tx_bytes);
-        tma_load_2d(dst, &tmA, k0, tile.row0, &sm->raw_full[s]);
-        tma_load_2d(dst + kM * C::RAW_ROW, &tmB, k0, tile.col0, &sm->raw_full[s]);
-        tma_load_2d(dst + (kM + kNB) * C::RAW_ROW, &tmW, k0, 0, &sm->raw_full[s]);
+#pragma unroll
+        for (int j = 0; j < C::A_BOXES; ++j)
+          tma_load_2d(dst + j * (kM * 128), &tmA, k0 + 32 * j, tile.row0, &sm->raw_full[s]);
+        tma_load_2d(dst + C::A_BYTES, &tmB, k0, tile.col0, &sm->raw_full[s]);
+        tma_load_2d(dst + C::A_BYTES + C::B_BYTES, &tmW, k0, 0, &sm->raw_full[s]);
       }
     }
     __syncwarp();
-  } else if (warp >= kConvWarp0 && warp < kConvWarp0 + kConvWarps) {
-    // ------------------------------ converters -----------------------------
-    const int t = threadIdx.x - kConvWarp0 * 32;
+  } else if (warp >= kAConvWarp0 && warp < kBConvWarp0) {
+    // ---------------------------- A converters -----------------------------
+    // Thread = A row r = TMEM lane; its raw row segment sits in 128-byte
+    // swizzled boxes (16-byte chunk j of row r at r*128 + ((j ^ (r & 7)) << 4)).
+    const int quarter = warp & 3;
+    const int r = quarter * 32 + lane;
+    const uint32_t lane_base = uint32_t(quarter * 32) << 16;
     for (int c = 0; c < nch; ++c) {
       const int rs = c % RS, os = c % kOpStages;
       if (!mbar_wait(&sm->raw_full[rs], uint32_t(c / RS) & 1u, abort_flag, a.err)) break;
       if (!mbar_wait(&sm->op_empty[os], (uint32_t(c / kOpStages) & 1u) ^ 1u, abort_flag, a.err)) break;
+      tc_fence_after();
       const uint8_t* raw = sm->raw[rs];
-      const float* rw = reinterpret_cast<const float*>(raw + (kM + kNB) * C::RAW_ROW);
-      uint8_t* st = sm->op[os];
-      uint8_t* a_hi = st;
-      uint8_t* a_lo = st + kATileBytes;
-      uint8_t* b_hi = st + 2 * kATileBytes;
-      uint8_t* b_lo = b_hi + kBTileBytes;
-      // A: 128 rows x 8 operand chunks, unweighted
-#pragma unroll 2
-      for (int q = 0; q < (kM * 8) / kConvThreads; ++q) {
-        const int id = q * kConvThreads + t;
-        const int r = id >> 3, ch = id & 7;
-        float x[EPC];
-        if (tile.row0 + r < a.total_rows) {
-          const float4* src = reinterpret_cast<const float4*>(raw + r * C::RAW_ROW + ch * EPC * 4);
+      const uint32_t a_hi = tmem + lane_base + kColA + uint32_t(os * 64);
 #pragma unroll
-          for (int v = 0; v < EPC / 4; ++v) {
-            const float4 f = src[v];
-            x[4 * v] = f.x; x[4 * v + 1] = f.y; x[4 * v + 2] = f.z; x[4 * v + 3] = f.w;
+      for (int half = 0; half < 2; ++half) {
+        // 16 TMEM columns: TF32 -> 16 samples, BF16 -> 32 samples (2 per column)
+        uint32_t hv[16], lv[16];
+        if (TF32) {
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const int j = half * 4 + q;
+            const float4 f = *reinterpret_cast<const float4*>(raw + r * 128 + ((j ^ (r & 7)) << 4));
+            const float x[4] = {f.x, f.y, f.z, f.w};
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+              hv[4 * q + e] = to_tf32_rn(x[e]);
+              lv[4 * q + e] = to_tf32_rn(x[e] - __uint_as_float(hv[4 * q + e]));
+            }
           }
         } else {
+          const uint8_t* box = raw + half * (kM * 128);
 #pragma unroll
-          for (int e = 0; e < EPC; ++e) x[e] = 0.f;
+          for (int q = 0; q < 8; ++q) {
+            const float4 f = *reinterpret_cast<const float4*>(box + r * 128 + ((q ^ (r & 7)) << 4));
+            const float x[4] = {f.x, f.y, f.z, f.w};
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+              const __nv_bfloat162 hb = __floats2bfloat162_rn(x[2 * e], x[2 * e + 1]);
+              const float2 hf = __bfloat1622float2(hb);
+              const __nv_bfloat162 lb = __floats2bfloat162_rn(x[2 * e] - hf.x, x[2 * e + 1] - hf.y);
+              hv[2 * q + e] = *reinterpret_cast<const uint32_t*>(&hb);
+              lv[2 * q + e] = *reinterpret_cast<const uint32_t*>(&lb);
+            }
+          }
         }
-        uint4 hi, lo;
-        if (TF32) split_tf32x4(x, hi, lo); else split_bf16x8(x, hi, lo);
-        const uint32_t off = sw128_off(r, ch);
-        *reinterpret_cast<uint4*>(a_hi + off) = hi;
-        *reinterpret_cast<uint4*>(a_lo + off) = lo;
+        tmem_st16(a_hi + half * 16, hv);
+        tmem_st16(a_hi + 32 + half * 16, lv);
       }
-      // B: 32 rows x 8 operand chunks x 3 weight planes
+      tmem_wait_st();
+      tc_fence_before();
+      mbar_arrive(&sm->op_full[os]);
+      mbar_arrive(&sm->raw_empty[rs]);
+    }
+  } else if (warp >= kBConvWarp0 && warp < kBConvWarp0 + 4) {
+    // ---------------------------- B converters -----------------------------
+    const int t = threadIdx.x - kBConvWarp0 * 32;
+    for (int c = 0; c < nch; ++c) {
+      const int rs = c % RS, os = c % kOpStages;
+      if (!mbar_wait(&sm->raw_full[rs], uint32_t(c / RS) & 1u, abort_flag, a.err)) break;
+      if (!mbar_wait(&sm->op_empty[os], (uint32_t(c / kOpStages) & 1u) ^ 1u, abort_flag, a.err)) break;
+      const uint8_t* rawb = sm->raw[rs] + C::A_BYTES;
+      const float* rw = reinterpret_cast<const float*>(sm->raw[rs] + C::A_BYTES + C::B_BYTES);
+      uint8_t* b_hi = sm->bop[os];
+      uint8_t* b_lo = b_hi + kBTileBytes;
+      // 32 rows x 8 operand chunks x 3 weight planes
 #pragma unroll 1
-      for (int q = 0; q < (kNB * 8) / kConvThreads; ++q) {
-        const int id = q * kConvThreads + t;
+      for (int q = 0; q < (kNB * 8) / 128; ++q) {
+        const int id = q * 128 + t;
         const int r = id >> 3, ch = id & 7;
         float x[EPC];
-        if (tile.col0 + r < a.total_rows) {
-          const float4* src = reinterpret_cast<const float4*>(raw + (kM + r) * C::RAW_ROW + ch * EPC * 4);
+        const float4* src = reinterpret_cast<const float4*>(rawb + r * C::RAW_ROW + ch * EPC * 4);
 #pragma unroll
-          for (int v = 0; v < EPC / 4; ++v) {
-            const float4 f = src[v];
-            x[4 * v] = f.x; x[4 * v + 1] = f.y; x[4 * v + 2] = f.z; x[4 * v + 3] = f.w;
-          }
-        } else {
-#pragma unroll
-          for (int e = 0; e < EPC; ++e) x[e] = 0.f;
+        for (int v = 0; v < EPC / 4; ++v) {
+          const float4 f = src[v];
+          x[4 * v] = f.x; x[4 * v + 1] = f.y; x[4 * v + 2] = f.z; x[4 * v + 3] = f.w;
         }
         const float* w0 = rw + ch * EPC;
         const float* w1 = rw + KC + ch * EPC;
@@ -412,40 +460,55 @@ gram_tc_kernel(const TcArgs a, const __grid_constant__ CUtensorMap tmA,
     }
   } else if (warp == kMmaWarp) {
     // ------------------------------ MMA issuer -----------------------------
+    // One thread issues every MMA, so its per-MMA instruction count bounds the
+    // tensor-core issue rate: all descriptors and TMEM addresses are formed
+    // once per stage, a K step only adds a constant, and the flush schedule is
+    // tracked with counters instead of divisions.
     if (lane == 0) {
-      bool ok = true;
-      for (int c = 0; c < nch && ok; ++c) {
-        const int s = c % kOpStages;
-        const int q = c / F;
-        const int b = q & 1;
-        if (c % F == 0) {
-          if (!mbar_wait(&sm->acc_empty[b], (uint32_t(q >> 1) & 1u) ^ 1u, abort_flag, a.err)) {
-            ok = false;
-            break;
-          }
+      const bool four = a.passes > 3;
+      static_assert(kOpStages == 2, "the issuer keeps one descriptor per operand stage");
+      const uint64_t bdesc0 = sw128_desc(smem_u32(sm->bop[0]));
+      const uint64_t bdesc1 = sw128_desc(smem_u32(sm->bop[1]));
+      constexpr uint64_t kLoDesc = uint64_t(kBTileBytes >> 4);  // B lo tile, in descriptor units
+      int s = 0, b = 0, f = 0;          // operand stage, hi*hi buffer, chunk within flush group
+      uint32_t ph_op = 0, ph_acc = 0;   // ph_acc bit b: phase of hi*hi buffer b
+      for (int c = 0; c < nch; ++c) {
+        if (f == 0) {
+          if (!mbar_wait(&sm->acc_empty[b], ((ph_acc >> b) & 1u) ^ 1u, abort_flag, a.err)) break;
+          ph_acc ^= 1u << b;
           tc_fence_after();
         }
-        if (!mbar_wait(&sm->op_full[s], uint32_t(c / kOpStages) & 1u, abort_flag, a.err)) {
-          ok = false;
-          break;
-        }
+        if (!mbar_wait(&sm->op_full[s], ph_op, abort_flag, a.err)) break;
         tc_fence_after();
-        const uint32_t base = smem_u32(sm->op[s]);
-        const uint32_t ahi = base, alo = base + kATileBytes;
-        const uint32_t bhi = base + 2 * kATileBytes, blo = bhi + kBTileBytes;
-        const uint32_t d = tmem + uint32_t(b * kBufCols);
-        const uint32_t dc = d + 128u;
+        const uint64_t bh = s ? bdesc1 : bdesc0, bl = bh + kLoDesc;
+        const uint32_t ahi = tmem + kColA + uint32_t(s * 64), alo = ahi + 32;
+        const uint32_t d = tmem + kColHH + uint32_t(b * 128);
+        const uint32_t dc = tmem + kColCorr;
+        const uint32_t acc_d = f == 0 ? 0u : 1u, acc_c = c == 0 ? 0u : 1u;
+        // K step ks: B advances 32 bytes (2 descriptor units), A 8 TMEM columns
+        mma_ts<TF32>(d, ahi, bh, IDESC, acc_d);
+        mma_ts<TF32>(dc, ahi, bl, IDESC, acc_c);
+        mma_ts<TF32>(dc, alo, bh, IDESC, 1u);
+        if (four) mma_ts<TF32>(dc, alo, bl, IDESC, 1u);
 #pragma unroll
-        for (int ks = 0; ks < NKSTEP; ++ks) {
-          const uint32_t o = ks * 32;
-          const uint32_t first = (c % F == 0 && ks == 0) ? 0u : 1u;
-          mma<TF32>(d, sw128_desc(ahi + o), sw128_desc(bhi + o), IDESC, first);
-          mma<TF32>(dc, sw128_desc(ahi + o), sw128_desc(blo + o), IDESC, first);
-          mma<TF32>(dc, sw128_desc(alo + o), sw128_desc(bhi + o), IDESC, 1u);
-          if (a.passes > 3) mma<TF32>(dc, sw128_desc(alo + o), sw128_desc(blo + o), IDESC, 1u);
+        for (int ks = 1; ks < NKSTEP; ++ks) {
+          mma_ts<TF32>(d, ahi + 8 * ks, bh + 2 * ks, IDESC, 1u);
+          mma_ts<TF32>(dc, ahi + 8 * ks, bl + 2 * ks, IDESC, 1u);
+          mma_ts<TF32>(dc, alo + 8 * ks, bh + 2 * ks, IDESC, 1u);
+          if (four) mma_ts<TF32>(dc, alo + 8 * ks, bl + 2 * ks, IDESC, 1u);
         }
         umma_commit(&sm->op_empty[s]);
-        if (c % F == F - 1 || c == nch - 1) umma_commit(&sm->acc_full[b]);
+        const bool last = (c == nch - 1);
+        if (++f == F || last) {
+          umma_commit(&sm->acc_full[b]);
+          f = 0;
+          b ^= 1;
+        }
+        if (last) umma_commit(&sm->corr_full);
+        if (++s == kOpStages) {
+          s = 0;
+          ph_op ^= 1u;
+        }
       }
       if (nch > 0) {
         // every issued MMA must retire before TMEM is released
@@ -460,38 +523,60 @@ gram_tc_kernel(const TcArgs a, const __grid_constant__ CUtensorMap tmA,
     const int part0 = (warp >> 2) * kEpiCols;  // first accumulator column of this thread
     // Plain FP32 running sums (round-to-nearest, unbiased): over n flushes the
     // relative rounding error is ~2^-24 sqrt(n) / 3 per split, and the FP64
-    // sum over splits averages it down further.  The flushed values are read
-    // eight columns at a time to stay within the register budget.
+    // sum over splits averages it down further.  Columns are read eight at a
+    // time to stay within the register budget.
     float sum[kEpiCols];
 #pragma unroll
     for (int i = 0; i < kEpiCols; ++i) sum[i] = 0.f;
     const uint32_t lane_base = uint32_t(quarter * 32) << 16;
+    bool ok = true;
     for (int q = 0; q < nint; ++q) {
       const int b = q & 1;
-      if (!mbar_wait(&sm->acc_full[b], uint32_t(q >> 1) & 1u, abort_flag, a.err)) break;
+      if (!mbar_wait(&sm->acc_full[b], uint32_t(q >> 1) & 1u, abort_flag, a.err)) {
+        ok = false;
+        break;
+      }
       tc_fence_after();
-      const uint32_t ta = tmem + lane_base + uint32_t(b * kBufCols + part0);
+      const uint32_t ta = tmem + lane_base + kColHH + uint32_t(b * 128 + part0);
 #pragma unroll
-      for (int part = 0; part < kEpiCols / 8; ++part) {
-        uint32_t hv[8], cv[8];
-        tmem_ld8(ta + part * 8, hv);
-        tmem_ld8(ta + 128 + part * 8, cv);
+      for (int part = 0; part < kEpiCols / 16; ++part) {
+        uint32_t v0[8], v1[8];
+        tmem_ld8(ta + part * 16, v0);
+        tmem_ld8(ta + part * 16 + 8, v1);
         tmem_wait_ld();
-        if (part == kEpiCols / 8 - 1) {
+        if (part == kEpiCols / 16 - 1) {
           // every column of this buffer is in registers: the MMAs may reuse it
           tc_fence_before();
           mbar_arrive(&sm->acc_empty[b]);
         }
 #pragma unroll
-        for (int i = 0; i < 8; ++i)
-          sum[part * 8 + i] += __uint_as_float(hv[i]) + __uint_as_float(cv[i]);
+        for (int i = 0; i < 8; ++i) {
+          sum[part * 16 + i] += __uint_as_float(v0[i]);
+          sum[part * 16 + 8 + i] += __uint_as_float(v1[i]);
+        }
       }
     }
-    if (!*(volatile int*)abort_flag && nint > 0) {
-      double* slot = a.partials + (size_t)tile.slot * (kM * kN) +
-                     (size_t)(quarter * 32 + lane) * kN + part0;
+    if (ok && nch > 0 && mbar_wait(&sm->corr_full, 0u, abort_flag, a.err)) {
+      tc_fence_after();
+      const uint32_t ta = tmem + lane_base + kColCorr + uint32_t(part0);
 #pragma unroll
-      for (int i = 0; i < kEpiCols; ++i) slot[i] += double(sum[i]);
+      for (int part = 0; part < kEpiCols / 16; ++part) {
+        uint32_t v0[8], v1[8];
+        tmem_ld8(ta + part * 16, v0);
+        tmem_ld8(ta + part * 16 + 8, v1);
+        tmem_wait_ld();
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          sum[part * 16 + i] += __uint_as_float(v0[i]);
+          sum[part * 16 + 8 + i] += __uint_as_float(v1[i]);
+        }
+      }
+      if (!*(volatile int*)abort_flag) {
+        double* slot = a.partials + (size_t)tile.slot * (kM * kN) +
+                       (size_t)(quarter * 32 + lane) * kN + part0;
+#pragma unroll
+        for (int i = 0; i < kEpiCols; ++i) slot[i] += double(sum[i]);
+      }
     }
   }
 
@@ -571,8 +656,10 @@ EncodeTiledFn encode_fn() {
 }
 
 // 2D FP32 map over a row-major [rows][ld] array, box = box_x samples x box_y rows,
-// no swizzle, rows past `rows` read as zero.
-bool make_map(CUtensorMap* m, const float* base, int ld, int rows, int box_x, int box_y) {
+// rows past `rows` read as zero; swizzle128 stores each 128-byte box row with
+// its 16-byte chunks XOR-permuted by (row % 8) (box_x must then be 32).
+bool make_map(CUtensorMap* m, const float* base, int ld, int rows, int box_x, int box_y,
+              bool swizzle128) {
   EncodeTiledFn fn = encode_fn();
   if (!fn) return false;
   const cuuint64_t dims[2] = {cuuint64_t(ld), cuuint64_t(rows)};
@@ -580,7 +667,8 @@ bool make_map(CUtensorMap* m, const float* base, int ld, int rows, int box_x, in
   const cuuint32_t box[2] = {cuuint32_t(box_x), cuuint32_t(box_y)};
   const cuuint32_t estr[2] = {1, 1};
   return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(base), dims, strides, box,
-            estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+            estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            swizzle128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE,
             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
@@ -590,9 +678,9 @@ int launch_t(const TcArgs& a, int n_jobs, cudaStream_t st) {
   if (smem > 227 * 1024) return LEMC_ERR_CAPACITY;
   constexpr int KC = Cfg<TF32>::KC;
   CUtensorMap tmA, tmB, tmW;
-  if (!make_map(&tmA, a.V, a.ldv, a.total_rows, KC, kM) ||
-      !make_map(&tmB, a.V, a.ldv, a.total_rows, KC, kNB) ||
-      !make_map(&tmW, a.rec_w, a.ldw, 3, KC, 3))
+  if (!make_map(&tmA, a.V, a.ldv, a.total_rows, 32, kM, true) ||
+      !make_map(&tmB, a.V, a.ldv, a.total_rows, KC, kNB, false) ||
+      !make_map(&tmW, a.rec_w, a.ldw, 3, KC, 3, false))
     return LEMC_ERR_CUDA;
   if (cudaFuncSetAttribute(gram_tc_kernel<TF32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            int(smem)) != cudaSuccess)
