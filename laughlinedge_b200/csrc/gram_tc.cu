@@ -251,10 +251,13 @@ __device__ __forceinline__ void split_bf16x8(const float* x, uint4& hi, uint4& l
   lo = make_uint4(l[0], l[1], l[2], l[3]);
 }
 
+// x rounded to the nearest TF32 value (ties away from zero), as a 32-bit
+// pattern whose 13 low mantissa bits are zero.  Adding half a TF32 ulp to the
+// magnitude bits and truncating is that rounding for every finite x (a carry
+// into the exponent is the correct round-up; overflow gives infinity) and
+// runs as two integer ops at full ALU rate.
 __device__ __forceinline__ uint32_t to_tf32_rn(float x) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-  return r;
+  return (__float_as_uint(x) + 0x1000u) & 0xFFFFE000u;
 }
 
 // hi = x rounded to nearest TF32, lo = (x - hi) rounded to nearest TF32: both
