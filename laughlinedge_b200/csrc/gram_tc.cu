@@ -427,32 +427,41 @@ gram_tc_kernel(const TcArgs a, const __grid_constant__ CUtensorMap tmA,
       const float* rw = reinterpret_cast<const float*>(sm->raw[rs] + C::A_BYTES + C::B_BYTES);
       uint8_t* b_hi = sm->bop[os];
       uint8_t* b_lo = b_hi + kBTileBytes;
-      // 32 rows x 8 operand chunks x 3 weight planes
-#pragma unroll 1
-      for (int q = 0; q < (kNB * 8) / 128; ++q) {
-        const int id = q * 128 + t;
-        const int r = id >> 3, ch = id & 7;
-        float x[EPC];
-        const float4* src = reinterpret_cast<const float4*>(rawb + r * C::RAW_ROW + ch * EPC * 4);
+      // 32 rows x 8 operand chunks x 3 weight planes.  A thread's chunks share
+      // one column range (ch = t % 8), so the weight products are formed once
+      // per K-chunk and the independent chunks are interleaved.
+      constexpr int kItems = (kNB * 8) / 128;
+      const int ch = t & 7;
+      float ww[3][EPC];
+#pragma unroll
+      for (int e = 0; e < EPC; ++e) {
+        const float one = rw[ch * EPC + e];
+        ww[0][e] = one;
+        ww[1][e] = one * rw[KC + ch * EPC + e];
+        ww[2][e] = one * rw[2 * KC + ch * EPC + e];
+      }
+      float x[kItems][EPC];
+#pragma unroll
+      for (int q = 0; q < kItems; ++q) {
+        const int rb = (q * 128 + t) >> 3;
+        const float4* src = reinterpret_cast<const float4*>(rawb + rb * C::RAW_ROW + ch * EPC * 4);
 #pragma unroll
         for (int v = 0; v < EPC / 4; ++v) {
           const float4 f = src[v];
-          x[4 * v] = f.x; x[4 * v + 1] = f.y; x[4 * v + 2] = f.z; x[4 * v + 3] = f.w;
+          x[q][4 * v] = f.x; x[q][4 * v + 1] = f.y; x[q][4 * v + 2] = f.z; x[q][4 * v + 3] = f.w;
         }
-        const float* w0 = rw + ch * EPC;
-        const float* w1 = rw + KC + ch * EPC;
-        const float* w2 = rw + 2 * KC + ch * EPC;
+      }
 #pragma unroll
-        for (int h = 0; h < 3; ++h) {
+      for (int h = 0; h < 3; ++h) {
+#pragma unroll
+        for (int q = 0; q < kItems; ++q) {
+          const int rb = (q * 128 + t) >> 3;
           float y[EPC];
 #pragma unroll
-          for (int e = 0; e < EPC; ++e) {
-            const float one = w0[e];
-            y[e] = x[e] * (h == 0 ? one : (h == 1 ? one * w1[e] : one * w2[e]));
-          }
+          for (int e = 0; e < EPC; ++e) y[e] = x[q][e] * ww[h][e];
           uint4 hi, lo;
           if (TF32) split_tf32x4(y, hi, lo); else split_bf16x8(y, hi, lo);
-          const uint32_t off = sw128_off(h * kNB + r, ch);
+          const uint32_t off = sw128_off(h * kNB + rb, ch);
           *reinterpret_cast<uint4*>(b_hi + off) = hi;
           *reinterpret_cast<uint4*>(b_lo + off) = lo;
         }
