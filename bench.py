@@ -211,7 +211,7 @@ def run_ours(args, ws, rank, local):
     mode = gram_mode_id(args.gram or w["gram_mode"])
     seed = w["seed"] + 1000003 * rank
     cfg = L.SamplerConfig(N, m, W, step_sigma=w["sigma"], seed=seed, lanes_per_walker=-1,
-                          gram_mode=mode)
+                          gram_mode=mode, graph_batch=args.graph_batch)
     smp = L.Sampler(cfg, w["sectors"])
     smp.init_walkers()
     smp.run(args.burn, measure=False)
@@ -332,7 +332,7 @@ def run_ours(args, ws, rank, local):
         "config": {"workload": w["workload"], "particles": N, "inverse_filling": m,
                    "sectors": "0..12", "basis_states": D, "walkers_per_gpu": W,
                    "sigma": w["sigma"], "gram_mode": args.gram or w["gram_mode"],
-                   "lanes_per_walker": G,
+                   "lanes_per_walker": G, "graph_batch": args.graph_batch,
                    "l2": "inputs larger than L2 (V planes 143 MB per step)",
                    "parallelism": f"replicas x{ws} (walkers sharded, no collective)"},
         "tau_int": tau, "tau_int_each": list(st.tau_int_each), "acceptance": st.acceptance,
@@ -357,6 +357,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--gram", default=None, choices=["fp64", "bf16x3", "bf16x4", "tf32x3"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--graph-batch", type=int, default=32,
+                    help="measured sweeps per CUDA-graph replay in the timed run (0: direct launches)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

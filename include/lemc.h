@@ -82,7 +82,9 @@ typedef struct lemc_config {
   double radius_scale;      /* R of (z/R)^k in p_k; <= 0 selects sqrt(2 m N) */
   double init_radius;       /* walkers start uniform in this disk; <=0: sqrt(2mN) */
   int32_t gram_mode;        /* enum lemc_gram_mode                           */
-  int32_t reserved1;
+  int32_t graph_batch;      /* >0: measured sweeps run as CUDA-graph replays of this
+                               many sweeps (sweep, basis, contraction each); results
+                               are identical to direct launches.  0: direct launches */
   int32_t flush_every;      /* tcgen05 path: K-chunks per FP64 flush (0=auto) */
   int32_t profile;          /* 1: time each kernel family with CUDA events   */
 } lemc_config;

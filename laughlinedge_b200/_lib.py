@@ -39,7 +39,7 @@ class Config(C.Structure):
                 ("n_walkers", C.c_int32), ("lanes_per_walker", C.c_int32),
                 ("step_sigma", C.c_float), ("guide", C.c_int32), ("seed", C.c_uint64),
                 ("radius_scale", C.c_double), ("init_radius", C.c_double),
-                ("gram_mode", C.c_int32), ("reserved1", C.c_int32),
+                ("gram_mode", C.c_int32), ("graph_batch", C.c_int32),
                 ("flush_every", C.c_int32), ("profile", C.c_int32)]
 
 

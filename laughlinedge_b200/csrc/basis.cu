@@ -19,7 +19,7 @@ namespace {
 __global__ void __launch_bounds__(256)
 basis_kernel(const float2* __restrict__ rec_p, int W, int K, float pN,
              const BasisNode* __restrict__ prog, int n_nodes, float* __restrict__ V, int ldv,
-             double* __restrict__ series) {
+             double* __restrict__ series, const uint32_t* __restrict__ series_idx) {
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
   const bool live = w < W;
   float2 p[kMaxDegree + 1];
@@ -29,6 +29,7 @@ basis_kernel(const float2* __restrict__ rec_p, int W, int K, float pN,
     p[k + 1] = (live && k < K) ? rec_p[(size_t)k * W + w] : make_float2(0.f, 0.f);
 
   if (series) {
+    if (series_idx) series += 8 * size_t(*series_idx);
     __shared__ double red[8][8];
     float o[8];
 #pragma unroll
@@ -70,12 +71,13 @@ basis_kernel(const float2* __restrict__ rec_p, int W, int K, float pN,
 }  // namespace
 
 int launch_basis(const float2* rec_p, int W, int K, int N, const BasisNode* prog, int n_nodes,
-                 float* V, int ldv, double* series, cudaStream_t st) {
+                 float* V, int ldv, double* series, const uint32_t* series_idx, cudaStream_t st) {
   if (K > kMaxDegree) return LEMC_ERR_CAPACITY;
   const int threads = 256;
   const int blocks = (W + threads - 1) / threads;
   basis_kernel<<<blocks, threads, 0, st>>>(reinterpret_cast<const float2*>(rec_p), W, K,
-                                           float(N), prog, n_nodes, V, ldv, series);
+                                           float(N), prog, n_nodes, V, ldv, series,
+                                           series_idx);
   return cudaPeekAtLastError() == cudaSuccess ? LEMC_OK : LEMC_ERR_CUDA;
 }
 

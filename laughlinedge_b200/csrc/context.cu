@@ -152,6 +152,15 @@ struct lemc_ctx {
   double ms_sweep = 0, ms_basis = 0, ms_gram = 0;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   std::vector<cudaEvent_t> pev;  // per-step profiling events (profile mode)
+  // graph replay of measured sweeps (cfg.graph_batch > 0): device counters
+  // {sweep index, measurement index} advanced inside the graph, and the
+  // instantiated graph with the state it was captured for
+  DevBuf<uint32_t> d_ctr;
+  cudaGraphExec_t gexec = nullptr;
+  uint64_t version = 0;          // bumped by every setter that changes launch arguments
+  uint64_t graph_version = ~uint64_t(0);
+  int graph_steps = 0;
+  const double* graph_series = nullptr;
 };
 
 namespace {
@@ -327,7 +336,7 @@ int upload_guide(lemc_ctx* c) {
   return LEMC_OK;
 }
 
-int sweep_once(lemc_ctx* c, int n_sweeps, int measure) {
+SweepArgs sweep_args(const lemc_ctx* c, int n_sweeps, int measure) {
   SweepArgs a{};
   a.pos = c->pos.p;
   a.rec_p = c->rec_p.p;
@@ -353,7 +362,11 @@ int sweep_once(lemc_ctx* c, int n_sweeps, int measure) {
   a.guide = c->cfg.guide;
   a.n_probes = int(c->probes.size());
   for (int q = 0; q < a.n_probes; ++q) a.probes[q] = c->probes[q];
-  return launch_sweep(a, c->G, c->stream);
+  return a;
+}
+
+int sweep_once(lemc_ctx* c, int n_sweeps, int measure) {
+  return launch_sweep(sweep_args(c, n_sweeps, measure), c->G, c->stream);
 }
 
 int gram_step(lemc_ctx* c, const float* V, const float* rec_w, int ldw, int W, int mode) {
@@ -528,6 +541,7 @@ int lemc_create(const lemc_config* cfg, lemc_ctx** out) {
     return LEMC_ERR_ARG;
   if (cfg->guide != LEMC_GUIDE_LAUGHLIN && cfg->guide != LEMC_GUIDE_ROW) return LEMC_ERR_ARG;
   if (cfg->gram_mode < LEMC_GRAM_FP64 || cfg->gram_mode > LEMC_GRAM_TF32X3) return LEMC_ERR_ARG;
+  if (cfg->graph_batch < 0 || cfg->graph_batch > 4096) return LEMC_ERR_ARG;
   int ndev = 0;
   if (lemc_device_count(&ndev) != LEMC_OK) return LEMC_ERR_NODEVICE;
   lemc_ctx* c = new lemc_ctx();
@@ -588,6 +602,8 @@ int lemc_destroy(lemc_ctx* c) {
   for (auto& e : c->ev)
     if (e) cudaEventDestroy(e);
   for (auto& e : c->pev) cudaEventDestroy(e);
+  if (c->gexec) cudaGraphExecDestroy(c->gexec);
+  c->d_ctr.release();
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return LEMC_OK;
@@ -595,6 +611,7 @@ int lemc_destroy(lemc_ctx* c) {
 
 int lemc_set_sectors(lemc_ctx* c, const int32_t* sectors, int n) {
   if (!c || !sectors || n <= 0) return LEMC_ERR_ARG;
+  ++c->version;
   std::vector<int> sec(sectors, sectors + n);
   for (size_t i = 0; i < sec.size(); ++i) {
     if (sec[i] < 0 || sec[i] > kMaxDegree) return LEMC_ERR_CAPACITY;
@@ -634,6 +651,7 @@ int lemc_set_sectors(lemc_ctx* c, const int32_t* sectors, int n) {
 
 int lemc_set_guide_rows(lemc_ctx* c, const int32_t* rows, int n_rows) {
   if (!c) return LEMC_ERR_ARG;
+  ++c->version;
   if (!c->has_basis) return LEMC_ERR_STATE;
   c->walker_row.clear();
   if (rows && n_rows > 0) {
@@ -678,6 +696,7 @@ static int autotune_lanes(lemc_ctx* c) {
                               cudaMemcpyDeviceToDevice, c->stream));
   }
   c->G = bestG;
+  ++c->version;
   if (c->accepted.p) LEMC_CUDA(cudaMemsetAsync(c->accepted.p, 0, 4 * c->W, c->stream));
   LEMC_CUDA(cudaStreamSynchronize(c->stream));
   save.release();
@@ -732,6 +751,7 @@ int lemc_synchronize(lemc_ctx* c) {
 int lemc_set_step(lemc_ctx* c, float sigma) {
   if (!c || !(sigma > 0.f)) return LEMC_ERR_ARG;
   c->cfg.step_sigma = sigma;
+  ++c->version;
   return LEMC_OK;
 }
 
@@ -754,10 +774,61 @@ int lemc_run_hooked(lemc_ctx* c, int n_sweeps, lemc_step_hook hook, void* user) 
 
 int lemc_set_probes(lemc_ctx* c, const int32_t* l, int n) {
   if (!c || n < 0 || n > LEMC_MAX_PROBES || (n > 0 && !l)) return LEMC_ERR_ARG;
+  ++c->version;
   c->probes.assign(l, l + n);
   for (int q : c->probes)
     if (q < 0 || q > 1024) return LEMC_ERR_ARG;
   if (c->has_basis) LEMC_TRY(build_jobs(c));
+  return LEMC_OK;
+}
+
+// One measured sweep with every per-step value taken from the device counters
+// (sweep index ctr[0], measurement index ctr[1]), then the counters advance:
+// G of these are captured once into a CUDA graph and replayed.
+static int graph_step(lemc_ctx* c) {
+  SweepArgs a = sweep_args(c, 1, 1);
+  a.sweep0 = 0;
+  a.sweep_ctr = c->d_ctr.p;
+  LEMC_TRY(launch_sweep(a, c->G, c->stream));
+  LEMC_TRY(launch_basis(c->rec_p.p, c->W, c->K, c->N, c->prog.p, c->n_nodes, c->V.p, c->Wpad,
+                        c->series.p, c->d_ctr.p + 1, c->stream));
+  LEMC_TRY(gram_step(c, c->V.p, c->rec_w.p, c->Wpad, c->W, c->cfg.gram_mode));
+  return launch_advance_counters(c->d_ctr.p, c->stream);
+}
+
+// Instantiate (or reuse) the graph of G measured sweeps for the current state.
+static int ensure_graph(lemc_ctx* c, int G) {
+  if (c->gexec && c->graph_version == c->version && c->graph_steps == G &&
+      c->graph_series == c->series.p)
+    return LEMC_OK;
+  if (c->gexec) {
+    cudaGraphExecDestroy(c->gexec);
+    c->gexec = nullptr;
+  }
+  // everything the captured launches point at must exist before capture
+  LEMC_TRY(c->d_ctr.alloc(2));
+  if (c->cfg.guide != LEMC_GUIDE_ROW && c->cfg.gram_mode != LEMC_GRAM_FP64 && c->tc_tiles.empty())
+    LEMC_TRY(setup_tc(c));
+  cudaGraph_t g = nullptr;
+  LEMC_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed));
+  int st = LEMC_OK;
+  for (int i = 0; i < G && st == LEMC_OK; ++i) st = graph_step(c);
+  const cudaError_t ce = cudaStreamEndCapture(c->stream, &g);
+  if (st != LEMC_OK || ce != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    return st != LEMC_OK ? st : LEMC_ERR_CUDA;
+  }
+  const cudaError_t ie = cudaGraphInstantiate(&c->gexec, g, 0);
+  cudaGraphDestroy(g);
+  if (ie != cudaSuccess) {
+    c->gexec = nullptr;
+    cudaGetLastError();
+    return LEMC_ERR_CUDA;
+  }
+  c->graph_version = c->version;
+  c->graph_steps = G;
+  c->graph_series = c->series.p;
   return LEMC_OK;
 }
 
@@ -786,14 +857,28 @@ static int run_impl(lemc_ctx* c, int n_sweeps, int measure, lemc_step_hook hook,
       c->pev.push_back(e);
     }
   }
-  for (int s = 0; s < n_sweeps; ++s) {
+  int s0 = 0;
+  const int G = c->cfg.graph_batch;
+  if (G > 0 && !hook && !c->profile && n_sweeps >= G) {
+    // whole batches of G measured sweeps as one graph launch each
+    LEMC_TRY(ensure_graph(c, G));
+    const uint32_t h_ctr[2] = {uint32_t(c->sweeps), 0u};
+    LEMC_CUDA(cudaMemcpyAsync(c->d_ctr.p, h_ctr, sizeof(h_ctr), cudaMemcpyHostToDevice, c->stream));
+    const int reps = n_sweeps / G;
+    for (int r = 0; r < reps; ++r) LEMC_CUDA(cudaGraphLaunch(c->gexec, c->stream));
+    s0 = reps * G;
+    c->sweeps += uint64_t(s0);
+    c->meas += uint64_t(s0);
+  }
+  for (int s = s0; s < n_sweeps; ++s) {
     if (c->profile) LEMC_CUDA(cudaEventRecord(c->pev[4 * s], c->stream));
     LEMC_TRY(sweep_once(c, 1, 1));
     c->sweeps += 1;
     if (c->profile) LEMC_CUDA(cudaEventRecord(c->pev[4 * s + 1], c->stream));
     LEMC_TRY(launch_basis(c->rec_p.p, c->W, c->K, c->N, c->prog.p, c->n_nodes, c->V.p, c->Wpad,
-                          c->series.p + 8 * size_t(s), c->stream));
+                          c->series.p + 8 * size_t(s), nullptr, c->stream));
     if (hook) {
+      if (!c->hooked) ++c->version;
       c->hooked = true;
       const int hs = hook(user, reinterpret_cast<const float*>(c->pos.p),
                           c->rec_w.p + size_t(LEMC_W_USER) * c->Wpad, c->W, c->N,
@@ -997,7 +1082,7 @@ int lemc_basis_device(lemc_ctx* c, const void* rec_p, int W, void* V, int ldv, v
   if (!c->has_basis) return LEMC_ERR_STATE;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   LEMC_TRY(launch_basis(static_cast<const float2*>(rec_p), W, c->K, c->N, c->prog.p, c->n_nodes,
-                        static_cast<float*>(V), ldv, nullptr, st));
+                        static_cast<float*>(V), ldv, nullptr, nullptr, st));
   return order_after(c, st);
 }
 

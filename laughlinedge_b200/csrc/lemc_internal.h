@@ -25,6 +25,7 @@ struct SweepArgs {
   float sigma, invR;
   uint32_t seed_lo, seed_hi;
   uint32_t sweep0;
+  const uint32_t* sweep_ctr;  // if set, *sweep_ctr is added to sweep0 (graph replay)
   int n_sweeps;
   int measure;
   int guide;
@@ -67,8 +68,12 @@ bool sweep_config_ok(int lanes_per_walker, int N);
 int launch_init_walkers(float2* pos, int W, int N, float radius, uint32_t seed_lo,
                         uint32_t seed_hi, cudaStream_t st);
 
+// series_idx (may be null): the walker-mean series goes to series + 8 * *series_idx
 int launch_basis(const float2* rec_p, int W, int K, int N, const BasisNode* prog,
-                 int n_nodes, float* V, int ldv, double* series, cudaStream_t st);
+                 int n_nodes, float* V, int ldv, double* series, const uint32_t* series_idx,
+                 cudaStream_t st);
+// ctr[0] += 1, ctr[1] += 1: sweep and measurement counters of a replayed graph
+int launch_advance_counters(uint32_t* ctr, cudaStream_t st);
 
 int launch_gram_simt(const float* V, int ldv, const float* rec_w, int ldw, int W,
                      const GramJob* jobs, int n_jobs, int n_splits, double* out_set0,

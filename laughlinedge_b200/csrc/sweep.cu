@@ -110,9 +110,10 @@ sweep_kernel(const SweepArgs a) {
   const float invR = a.invR;
   const float mf = float(a.m);
   uint32_t nacc = 0;
+  const uint32_t sweep_base = a.sweep0 + (a.sweep_ctr ? *a.sweep_ctr : 0u);
 
   for (int s = 0; s < a.n_sweeps; ++s) {
-    const uint32_t sweep = a.sweep0 + uint32_t(s);
+    const uint32_t sweep = sweep_base + uint32_t(s);
     // refresh the guide power sums from the positions (bounds FP drift)
     if (row_guide) {
 #pragma unroll
@@ -368,6 +369,18 @@ int launch_init_walkers(float2* pos, int W, int N, float radius, uint32_t k0, ui
   const int threads = 256;
   const unsigned blocks = unsigned((n + threads - 1) / threads);
   init_walkers_kernel<<<blocks, threads, 0, st>>>(pos, W, N, radius, k0, k1);
+  return cudaPeekAtLastError() == cudaSuccess ? LEMC_OK : LEMC_ERR_CUDA;
+}
+
+namespace {
+__global__ void advance_counters_kernel(uint32_t* ctr) {
+  ctr[0] += 1u;
+  ctr[1] += 1u;
+}
+}  // namespace
+
+int launch_advance_counters(uint32_t* ctr, cudaStream_t st) {
+  advance_counters_kernel<<<1, 1, 0, st>>>(ctr);
   return cudaPeekAtLastError() == cudaSuccess ? LEMC_OK : LEMC_ERR_CUDA;
 }
 

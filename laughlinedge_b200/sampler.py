@@ -116,13 +116,14 @@ class SamplerConfig:
     init_radius: float = 0.0
     gram_mode: int = _lib.GRAM_FP64
     flush_every: int = 0
+    graph_batch: int = 0
     profile: bool = False
 
     def to_c(self) -> _lib.Config:
         return _lib.Config(self.particles, self.inverse_filling, self.n_walkers,
                            self.lanes_per_walker, self.step_sigma, self.guide, self.seed,
                            self.radius_scale, self.init_radius, self.gram_mode,
-                           0, self.flush_every, 1 if self.profile else 0)
+                           self.graph_batch, self.flush_every, 1 if self.profile else 0)
 
 
 class Sampler:
