@@ -297,6 +297,20 @@ LEMC_API int lemc_occupation_static(const lemc_occupation_config* cfg, double* o
 LEMC_API int lemc_geneig(int D, const double* H, const double* M, double eps,
                 double* evals, double* evecs, int* rank);
 
+/* Generalized spectra of one sector for n confinement strengths, computed on
+ * the GPU in FP64 (the kappa sweep of the batched form).  S, H2, H4 are the raw
+ * Gram sums of lemc_read_gram (D x D complex, interleaved); for each j the
+ * problem is H_j c = E M c with M and H_j normalised and Hermitised as in
+ * lemc_normalise, H_j = omega[j] H2 + kappa[j] H4.  M is factorised once by
+ * canonical orthogonalisation: directions with metric eigenvalue <= eps * max
+ * are dropped (*rank = kept dimension; evals beyond it are NaN).
+ * evals[j*D + k] ascending.  Replaces ges::generalizedEigenproblem
+ * (modules/eigensolver/generalized_eigenproblem.cpp:38-95) called once per
+ * strength. */
+LEMC_API int lemc_geneig_sweep(int D, const double* S, const double* H2, const double* H4,
+                               const double* omega, const double* kappa, int n, double eps,
+                               double* evals, int* rank);
+
 /* Normalised matrices from raw Gram sums (reference convention,
  * em_spectrum.cu:331-335 and the Hermitisation at :383-390):
  *   M[a][b] = S[a][b] / sqrt(S[a][a] S[b][b]),

@@ -5,7 +5,8 @@ sm_100a behind the C-ABI of include/lemc.h); this package only binds it.
 """
 from . import _lib
 from ._lib import LemcError, load
-from .sampler import Sampler, SamplerConfig, evolve, geneig, normalise, partitions
+from .sampler import (Sampler, SamplerConfig, evolve, geneig, geneig_sweep, normalise,
+                      partitions)
 
-__all__ = ["LemcError", "Sampler", "SamplerConfig", "evolve", "geneig", "load", "normalise",
-           "partitions", "_lib"]
+__all__ = ["LemcError", "Sampler", "SamplerConfig", "evolve", "geneig", "geneig_sweep", "load",
+           "normalise", "partitions", "_lib"]

@@ -105,6 +105,7 @@ _SIGNATURES = {
     "lemc_basis_device": ([_P, _P, _I, _P, _I, _P], _I),
     "lemc_gram_device": ([_P, _P, _P, _I, _I, _I, _P], _I),
     "lemc_geneig": ([_I, _DP, _DP, _D, _DP, _DP, _IP], _I),
+    "lemc_geneig_sweep": ([_I, _DP, _DP, _DP, _DP, _DP, _I, _D, _DP, _IP], _I),
     "lemc_normalise": ([_I, _DP, _DP, _DP, _D, _D, _DP, _DP], _I),
     "lemc_evolve": ([_I, _DP, _DP, _DP, _I, _DP, PROFILE_FN, _P, _D, _D, _DP, _DP, _IP], _I),
 }

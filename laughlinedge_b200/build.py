@@ -65,7 +65,7 @@ def build(verbose: bool = False, force: bool = False) -> Path:
         objs = list(ex.map(lambda s: _compile(s, hdr_time, verbose), srcs))
     if LIB.exists() and LIB.stat().st_mtime >= _newest(objs) and not force:
         return LIB
-    cmd = [NVCC] + ARCH + ["-shared", "-o", str(LIB)] + [str(o) for o in objs] + ["-lcudart"]
+    cmd = [NVCC] + ARCH + ["-shared", "-o", str(LIB)] + [str(o) for o in objs] + ["-lcudart", "-lcusolver", "-lcublas"]
     if verbose:
         print(" ".join(cmd), flush=True)
     r = subprocess.run(cmd, capture_output=True, text=True)

@@ -57,6 +57,23 @@ def geneig(H: np.ndarray, M: np.ndarray, eps: float = 1e-12, vectors: bool = Fal
     return ev
 
 
+def geneig_sweep(S, H2, H4, omegas, kappas, eps: float = 1e-12):
+    """Generalized spectra of one sector for many (omega, kappa), FP64 on the GPU.
+
+    Returns (evals [n, D] ascending, NaN beyond the kept rank; rank)."""
+    lib = _lib.load()
+    D = S.shape[0]
+    om = np.ascontiguousarray(omegas, dtype=np.float64)
+    ka = np.ascontiguousarray(kappas, dtype=np.float64)
+    assert om.shape == ka.shape and om.ndim == 1
+    buf = [np.ascontiguousarray(X, dtype=np.complex128).view(np.float64).ravel() for X in (S, H2, H4)]
+    ev = np.zeros(len(om) * D)
+    rank = C.c_int()
+    check(lib.lemc_geneig_sweep(D, dptr(buf[0]), dptr(buf[1]), dptr(buf[2]), dptr(om), dptr(ka),
+                                len(om), eps, dptr(ev), C.byref(rank)), "lemc_geneig_sweep")
+    return ev.reshape(len(om), D), rank.value
+
+
 def normalise(S, H2=None, H4=None, omega=0.0, kappa=0.0):
     """Reference normalisation M = S/sqrt(S_aa S_bb), H = (w H2 + k H4)/sqrt(..), Hermitised."""
     lib = _lib.load()

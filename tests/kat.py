@@ -72,6 +72,30 @@ def gram_m1(N, rows, R=1.0):
     return (X * np.array(w)) @ X.T / R ** (2 * n)
 
 
+def gram_m1_weighted(N, rows, R=1.0):
+    """Exact (sum r^2)- and (sum r^4)-weighted Gram matrices of the rows at nu = 1.
+
+    The Schur states s_mu Psi_1 are Slater determinants of the orbitals
+    n_j = mu_j + N - j (j = 1..N), and sum_i |z_i|^2, sum_i |z_i|^4 are diagonal
+    in them with values sum_j 2(n_j+1) and sum_j 4(n_j+1)(n_j+2); the weighted
+    Gram matrices are gram_m1 with those factors inside the character sum."""
+    lams = [row_to_desc(pr) for _, pr in rows]
+    n = sum(lams[0])
+    mus = [mu for mu in partitions_desc(n) if len(mu) <= N]
+    w, w2, w4 = [], [], []
+    for mu in mus:
+        v = 1.0
+        for j, mj in enumerate(mu, start=1):
+            v *= 2.0 ** mj * factorial(mj + N - j) / factorial(N - j)
+        ns = [(mu[j] if j < len(mu) else 0) + N - 1 - j for j in range(N)]
+        w.append(v)
+        w2.append(v * sum(2.0 * (x + 1) for x in ns))
+        w4.append(v * sum(4.0 * (x + 1) * (x + 2) for x in ns))
+    X = np.array([[character(mu, lam) for mu in mus] for lam in lams], dtype=float)
+    sc = R ** (2 * n)
+    return (X * np.array(w2)) @ X.T / sc, (X * np.array(w4)) @ X.T / sc
+
+
 def spectrum_m1(N, dL, omega, kappa):
     out = []
     for mu in partitions_desc(dL):

@@ -89,3 +89,14 @@ def test_evolve_matches_scipy(lemc):
         for l, r in enumerate(rho):
             assert abs(out[s, l] - c.conj() @ r @ c) < 1e-6 * (1 + abs(c.conj() @ r @ c))
         assert abs(norms[s] - (c.conj() @ M @ c).real) < 1e-6 * norms[0]
+
+
+def test_geneig_m1_closed_form_spectrum(lemc):
+    """Host solver on the exact nu = 1 Gram matrices: E_mu in closed form."""
+    import kat
+    N, dL = 6, 5
+    rows = lemc.partitions(N, [dL])[0]
+    S = kat.gram_m1(N, rows).astype(complex)
+    H2, H4 = kat.gram_m1_weighted(N, rows)
+    M, H = lemc.normalise(S, H2.astype(complex), H4.astype(complex), 1e-2, 1e-4)
+    np.testing.assert_allclose(lemc.geneig(H, M), kat.spectrum_m1(N, dL, 1e-2, 1e-4), rtol=1e-9)
