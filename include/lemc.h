@@ -235,6 +235,57 @@ LEMC_API int lemc_basis_device(lemc_ctx* ctx, const void* rec_p, int W, void* V,
 LEMC_API int lemc_gram_device(lemc_ctx* ctx, const void* V, const void* rec_w, int W,
                      int ldv, int gram_mode, void* stream);
 
+/* ---- learned proposal (DeepSets network, exact Metropolis-Hastings) ---------
+ * No counterpart in the reference, whose sampler moves one particle by an
+ * isotropic Gaussian step.  A lemc_proposal holds the weights of a small
+ * permutation-invariant network: the 16 nearest-neighbour displacements of
+ * the moving particle in its local radial/tangential frame -> phi (2 -> 64,
+ * ReLU) -> mean, with r/R - 1 appended -> rho (65 -> 64, ReLU -> 4) =
+ * (mu_r, mu_t, log s_r, log s_t) of the proposed move z' = z + Rot(theta)(mu
+ * + s eps).  A context using it (lemc_set_proposal) accepts with the exact
+ * ratio |Psi(z')|^2 q(z|z') / (|Psi(z)|^2 q(z'|z)), so it samples |Psi_m|^2
+ * for any weights.  Weights: FP32 master copy, BF16 copy used by the kernels.
+ * particles <= 256; Laughlin guide only. */
+typedef struct lemc_proposal lemc_proposal;
+typedef struct lemc_train_config {
+  int32_t steps;      /* Adam steps */
+  int32_t batch;      /* (configuration, particle, eps) samples per objective estimate */
+  int32_t pairs;      /* antithetic parameter perturbations per step */
+  float lr;           /* Adam learning rate */
+  float es_sigma;     /* perturbation scale of the evolution-strategies gradient */
+  uint64_t seed;      /* Philox key of samples and perturbations */
+} lemc_train_config;
+/* Number of network parameters (FP32 layout W1[64][2], b1[64], W2[64][65], b2[64],
+ * W3[4][64], b3[4]). */
+LEMC_API int lemc_proposal_n_params(int* n);
+/* New proposal initialised to the plain isotropic step init_sigma (hidden
+ * weights random from seed, output weights near zero). */
+LEMC_API int lemc_proposal_create(int particles, int inverse_filling, float init_sigma,
+                                  uint64_t seed, lemc_proposal** out);
+LEMC_API int lemc_proposal_destroy(lemc_proposal* p);
+LEMC_API int lemc_proposal_get_params(const lemc_proposal* p, float* host, int n);
+/* Replace the weights (also resets the Adam state). */
+LEMC_API int lemc_proposal_set_params(lemc_proposal* p, const float* host, int n);
+/* For n (configuration, particle, eps) samples (host arrays: xy [n][particles][2],
+ * particle [n], eps [n][2]) write out[s][8] = {mu_r, mu_t, log s_r, log s_t,
+ * z'.x, z'.y, ln A, |z'-z|^2} as the sampler computes them (BF16 weights). */
+LEMC_API int lemc_proposal_eval(const lemc_proposal* p, const float* host_xy, int n,
+                                const int32_t* particle, const float* eps, float* out);
+/* Maximise E[min(1, A) |z'-z|^2] over configurations `configs` (device array
+ * [n_cfg][particles] of float2, e.g. snapshots of a plain-proposal context via
+ * lemc_copy_positions_device): per step 2*pairs antithetic weight
+ * perturbations evaluated on `batch` common samples give an
+ * evolution-strategies gradient for one Adam step.  trace[s] (host, may be NULL)
+ * receives the mean objective of step s. */
+LEMC_API int lemc_proposal_train(lemc_proposal* p, const void* configs, int n_cfg,
+                                 const lemc_train_config* cfg, double* trace);
+/* Use proposal p for the context's sweeps (NULL: the plain Gaussian step).
+ * p must outlive its use; particles and inverse filling must match. */
+LEMC_API int lemc_set_proposal(lemc_ctx* ctx, const lemc_proposal* p);
+/* Copy the context's walker positions ([W][N] float2) to device memory dst,
+ * ordered on the context stream. */
+LEMC_API int lemc_copy_positions_device(lemc_ctx* ctx, void* dst);
+
 /* ---- occupation numbers (two-state walker) -------------------------------
  * <f_L| a^dagger_l a_l |f_R> for every ordered pair (L, R) of basis rows of
  * sector dL, l < l_cutoff.  Each walker carries N+1 particles: particle 0

@@ -56,6 +56,11 @@ class OccConfig(C.Structure):
                 ("seed", C.c_uint64), ("burn_in", C.c_int32), ("sweeps", C.c_int32)]
 
 
+class TrainConfig(C.Structure):
+    _fields_ = [("steps", C.c_int32), ("batch", C.c_int32), ("pairs", C.c_int32),
+                ("lr", C.c_float), ("es_sigma", C.c_float), ("seed", C.c_uint64)]
+
+
 class PartitionRow(C.Structure):
     _fields_ = [("dL", C.c_int32), ("sector_size", C.c_int32), ("n_pairs", C.c_int32),
                 ("pairs_off", C.c_int32)]
@@ -105,6 +110,15 @@ _SIGNATURES = {
     "lemc_basis_device": ([_P, _P, _I, _P, _I, _P], _I),
     "lemc_gram_device": ([_P, _P, _P, _I, _I, _I, _P], _I),
     "lemc_geneig": ([_I, _DP, _DP, _D, _DP, _DP, _IP], _I),
+    "lemc_proposal_n_params": ([_IP], _I),
+    "lemc_proposal_create": ([_I, _I, C.c_float, C.c_uint64, C.POINTER(_P)], _I),
+    "lemc_proposal_destroy": ([_P], _I),
+    "lemc_proposal_get_params": ([_P, _FP, _I], _I),
+    "lemc_proposal_set_params": ([_P, _FP, _I], _I),
+    "lemc_proposal_eval": ([_P, _FP, _I, _I32P, _FP, _FP], _I),
+    "lemc_proposal_train": ([_P, _P, _I, C.POINTER(TrainConfig), _DP], _I),
+    "lemc_set_proposal": ([_P, _P], _I),
+    "lemc_copy_positions_device": ([_P, _P], _I),
     "lemc_geneig_sweep": ([_I, _DP, _DP, _DP, _DP, _DP, _I, _D, _DP, _IP], _I),
     "lemc_normalise": ([_I, _DP, _DP, _DP, _D, _D, _DP, _DP], _I),
     "lemc_evolve": ([_I, _DP, _DP, _DP, _I, _DP, PROFILE_FN, _P, _D, _D, _DP, _DP, _IP], _I),

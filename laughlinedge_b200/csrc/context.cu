@@ -156,6 +156,7 @@ struct lemc_ctx {
   // {sweep index, measurement index} advanced inside the graph, and the
   // instantiated graph with the state it was captured for
   DevBuf<uint32_t> d_ctr;
+  const lemc_proposal* prop = nullptr;  // learned proposal (null: Gaussian step)
   cudaGraphExec_t gexec = nullptr;
   uint64_t version = 0;          // bumped by every setter that changes launch arguments
   uint64_t graph_version = ~uint64_t(0);
@@ -365,8 +366,13 @@ SweepArgs sweep_args(const lemc_ctx* c, int n_sweeps, int measure) {
   return a;
 }
 
+int launch_sweep_for(lemc_ctx* c, const SweepArgs& a) {
+  if (c->prop) return launch_learned_sweep(a, lemc_proposal_weights(c->prop), c->stream);
+  return launch_sweep(a, c->G, c->stream);
+}
+
 int sweep_once(lemc_ctx* c, int n_sweeps, int measure) {
-  return launch_sweep(sweep_args(c, n_sweeps, measure), c->G, c->stream);
+  return launch_sweep_for(c, sweep_args(c, n_sweeps, measure));
 }
 
 int gram_step(lemc_ctx* c, const float* V, const float* rec_w, int ldw, int W, int mode) {
@@ -755,6 +761,24 @@ int lemc_set_step(lemc_ctx* c, float sigma) {
   return LEMC_OK;
 }
 
+int lemc_set_proposal(lemc_ctx* c, const lemc_proposal* p) {
+  if (!c) return LEMC_ERR_ARG;
+  if (p) {
+    if (lemc_proposal_particles(p) != c->N || lemc_proposal_filling(p) != c->m) return LEMC_ERR_ARG;
+    if (c->cfg.guide != LEMC_GUIDE_LAUGHLIN) return LEMC_ERR_ARG;
+  }
+  c->prop = p;
+  ++c->version;
+  return LEMC_OK;
+}
+
+int lemc_copy_positions_device(lemc_ctx* c, void* dst) {
+  if (!c || !dst) return LEMC_ERR_ARG;
+  LEMC_CUDA(cudaMemcpyAsync(dst, c->pos.p, sizeof(float2) * size_t(c->W) * c->N,
+                            cudaMemcpyDeviceToDevice, c->stream));
+  return LEMC_OK;
+}
+
 int lemc_stream(lemc_ctx* c, void** stream) {
   if (!c || !stream) return LEMC_ERR_ARG;
   *stream = static_cast<void*>(c->stream);
@@ -789,7 +813,7 @@ static int graph_step(lemc_ctx* c) {
   SweepArgs a = sweep_args(c, 1, 1);
   a.sweep0 = 0;
   a.sweep_ctr = c->d_ctr.p;
-  LEMC_TRY(launch_sweep(a, c->G, c->stream));
+  LEMC_TRY(launch_sweep_for(c, a));
   LEMC_TRY(launch_basis(c->rec_p.p, c->W, c->K, c->N, c->prog.p, c->n_nodes, c->V.p, c->Wpad,
                         c->series.p, c->d_ctr.p + 1, c->stream));
   LEMC_TRY(gram_step(c, c->V.p, c->rec_w.p, c->Wpad, c->W, c->cfg.gram_mode));

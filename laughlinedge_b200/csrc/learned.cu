@@ -1,0 +1,624 @@
+// Learned Metropolis-Hastings proposal for the Laughlin target (sm_100a).
+//
+// A small permutation-invariant network proposes the single-particle move:
+// for particle i at z_i, the displacements to its 16 nearest other particles,
+// rotated into the local (radial, tangential) frame of z_i and scaled by 1/2,
+// pass through phi (2 -> 64, ReLU); their mean, with r_i/R - 1 appended,
+// passes through rho (65 -> 64, ReLU -> 4) giving (mu_r, mu_t, log s_r, log s_t)
+// of an axis-aligned Gaussian in that frame:
+//   z' = z_i + Rot(theta_i) (mu + s * eps),   eps ~ N(0, 1)^2.
+// The acceptance is the exact Metropolis-Hastings ratio
+//   A = |Psi(z')|^2 q(z | z') / (|Psi(z)|^2 q(z' | z)),
+// where q(z | z') is the same network evaluated at the proposed configuration
+// (its own neighbours and frame), so the chain samples |Psi_m|^2 exactly
+// whatever the weights are.  Weights are stored in BF16, arithmetic is FP32.
+//
+// Sampler layout: one walker per warp, positions in shared memory, lane l
+// owns particles l, l+32, ...  The 16 neighbours are found in 16 rounds of a
+// warp-wide minimum (redux.sync) over packed (distance^2, index) keys; each
+// lane evaluates two of the 64 hidden units of each layer; every reduction is
+// an xor butterfly, so all lanes hold bitwise identical values and take the
+// same accept decision.  Random numbers: Philox {i, sweep, walker, 4}.
+//
+// Training (evolution strategies + Adam, forward-only kernels): the objective
+// J = E[min(1, A) |z' - z_i|^2] over (configuration, particle, eps) samples
+// is estimated for 2P antithetic parameter perturbations with common random
+// numbers; the ES gradient drives an Adam step on FP32 master weights.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <random>
+#include <vector>
+
+#include "lemc_internal.h"
+#include "lemc_rng.h"
+
+namespace lemc {
+namespace {
+
+constexpr int kH = 64;      // hidden width
+constexpr int kNbr = 16;    // neighbours
+constexpr int kIn = kH + 1; // rho input: mean(phi) and r/R - 1
+constexpr int kOffW1 = 0;                  // [kH][2]
+constexpr int kOffB1 = kOffW1 + kH * 2;    // [kH]
+constexpr int kOffW2 = kOffB1 + kH;        // [kH][kIn]
+constexpr int kOffB2 = kOffW2 + kH * kIn;  // [kH]
+constexpr int kOffW3 = kOffB2 + kH;        // [4][kH]
+constexpr int kOffB3 = kOffW3 + 4 * kH;    // [4]
+constexpr int kNParams = kOffB3 + 4;
+constexpr float kInScale = 0.5f;           // displacement feature scale (1 / 2 l_B)
+constexpr float kLogSMin = -3.912023f;     // log 0.02
+constexpr float kLogSMax = 1.386294f;      // log 4
+constexpr int kMaxN = 256;                 // packed kNN keys carry 8 index bits
+constexpr int kSlots = kMaxN / 32;         // particles per lane
+constexpr uint32_t kTagLearned = 4u, kTagTrain = 5u, kTagEs = 6u;
+constexpr int kWarpsPerBlock = 4;   // sampler / evaluation blocks
+constexpr int kTrainWarps = 16;     // ES blocks share one perturbed weight set
+constexpr float kLn2 = 0.6931471805599453f;
+
+struct NetOut {
+  float mr, mt, lr, lt;
+};
+
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// The network at centre zc for particle `self` of the walker whose positions
+// are zs[0..N).  All 32 lanes call it; every lane returns the same values.
+__device__ NetOut net_eval(const float* __restrict__ P, const float2* zs, int N, int self,
+                           float2 zc, float invR, int lane) {
+  const float r2 = zc.x * zc.x + zc.y * zc.y;
+  float c = 1.f, s = 0.f;
+  if (r2 > 1e-20f) {
+    const float ri = rsqrtf(r2);
+    c = zc.x * ri;
+    s = zc.y * ri;
+  }
+  uint32_t key[kSlots];
+#pragma unroll
+  for (int t = 0; t < kSlots; ++t) {
+    const int j = lane + 32 * t;
+    key[t] = 0xFFFFFFFFu;
+    if (j < N && j != self) {
+      const float dx = zs[j].x - zc.x, dy = zs[j].y - zc.y;
+      key[t] = (__float_as_uint(fmaf(dx, dx, dy * dy)) & 0xFFFFFF00u) | uint32_t(j);
+    }
+  }
+  const float w0x = P[kOffW1 + 2 * lane], w0y = P[kOffW1 + 2 * lane + 1], b0 = P[kOffB1 + lane];
+  const float w1x = P[kOffW1 + 2 * (lane + 32)], w1y = P[kOffW1 + 2 * (lane + 32) + 1];
+  const float b1 = P[kOffB1 + lane + 32];
+  float g0 = 0.f, g1 = 0.f;
+  int cnt = 0;
+  for (int n = 0; n < kNbr; ++n) {
+    uint32_t lm = key[0];
+#pragma unroll
+    for (int t = 1; t < kSlots; ++t) lm = min(lm, key[t]);
+    const uint32_t m = __reduce_min_sync(0xffffffffu, lm);
+    if (m == 0xFFFFFFFFu) break;
+#pragma unroll
+    for (int t = 0; t < kSlots; ++t)
+      if (key[t] == m) key[t] = 0xFFFFFFFFu;
+    const int j = int(m & 0xFFu);
+    const float dx = zs[j].x - zc.x, dy = zs[j].y - zc.y;
+    const float xr = (dx * c + dy * s) * kInScale, xt = (dy * c - dx * s) * kInScale;
+    g0 += fmaxf(fmaf(w0x, xr, fmaf(w0y, xt, b0)), 0.f);
+    g1 += fmaxf(fmaf(w1x, xr, fmaf(w1y, xt, b1)), 0.f);
+    ++cnt;
+  }
+  if (cnt > 0) {
+    const float inv = 1.f / float(cnt);
+    g0 *= inv;
+    g1 *= inv;
+  }
+  const float sf = sqrtf(r2) * invR - 1.f;
+  const float* w2a = P + kOffW2 + lane * kIn;
+  const float* w2b = P + kOffW2 + (lane + 32) * kIn;
+  float k0 = fmaf(w2a[kH], sf, P[kOffB2 + lane]);
+  float k1 = fmaf(w2b[kH], sf, P[kOffB2 + lane + 32]);
+#pragma unroll 8
+  for (int v = 0; v < 32; ++v) {
+    const float ga = __shfl_sync(0xffffffffu, g0, v), gb = __shfl_sync(0xffffffffu, g1, v);
+    k0 = fmaf(w2a[v], ga, fmaf(w2a[v + 32], gb, k0));
+    k1 = fmaf(w2b[v], ga, fmaf(w2b[v + 32], gb, k1));
+  }
+  k0 = fmaxf(k0, 0.f);
+  k1 = fmaxf(k1, 0.f);
+  float o[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+    o[q] = warp_sum(fmaf(P[kOffW3 + q * kH + lane], k0, P[kOffW3 + q * kH + lane + 32] * k1)) +
+           P[kOffB3 + q];
+  return NetOut{o[0], o[1], fminf(fmaxf(o[2], kLogSMin), kLogSMax),
+                fminf(fmaxf(o[3], kLogSMin), kLogSMax)};
+}
+
+// Everything one proposed move needs, identical on all lanes.
+struct Move {
+  float2 zn;       // proposed position
+  float log_a;     // natural log of the Metropolis-Hastings ratio
+  float jump2;     // |z' - z|^2
+};
+
+__device__ Move propose(const float* __restrict__ P, const float2* zs, int N, int i, float invR,
+                        float m, float e_r, float e_t, int lane) {
+  const float2 zo = zs[i];
+  const NetOut f = net_eval(P, zs, N, i, zo, invR, lane);
+  const float sr = __expf(f.lr), st = __expf(f.lt);
+  const float dr = fmaf(sr, e_r, f.mr), dt = fmaf(st, e_t, f.mt);
+  const float r2 = zo.x * zo.x + zo.y * zo.y;
+  float c = 1.f, s = 0.f;
+  if (r2 > 1e-20f) {
+    const float ri = rsqrtf(r2);
+    c = zo.x * ri;
+    s = zo.y * ri;
+  }
+  Move mv;
+  mv.zn = make_float2(zo.x + (c * dr - s * dt), zo.y + (s * dr + c * dt));
+  const float log_qf = -0.5f * (e_r * e_r + e_t * e_t) - f.lr - f.lt;
+  // reverse proposal: the network at the proposed configuration
+  const NetOut b = net_eval(P, zs, N, i, mv.zn, invR, lane);
+  const float rn2 = mv.zn.x * mv.zn.x + mv.zn.y * mv.zn.y;
+  float cb = 1.f, sb = 0.f;
+  if (rn2 > 1e-20f) {
+    const float ri = rsqrtf(rn2);
+    cb = mv.zn.x * ri;
+    sb = mv.zn.y * ri;
+  }
+  const float bx = zo.x - mv.zn.x, by = zo.y - mv.zn.y;
+  const float br = bx * cb + by * sb, bt = by * cb - bx * sb;
+  const float ur = (br - b.mr) * __expf(-b.lr), ut = (bt - b.mt) * __expf(-b.lt);
+  const float log_qb = -0.5f * (ur * ur + ut * ut) - b.lr - b.lt;
+  // target ratio: m sum_j ln(|z'-z_j|^2 / |z-z_j|^2) - (|z'|^2 - |z|^2) / 2
+  float lj = 0.f;
+#pragma unroll
+  for (int t = 0; t < kSlots; ++t) {
+    const int j = lane + 32 * t;
+    if (j < N && j != i) {
+      const float2 zj = zs[j];
+      const float ax = mv.zn.x - zj.x, ay = mv.zn.y - zj.y, ox = zo.x - zj.x, oy = zo.y - zj.y;
+      lj += __log2f(fmaf(ax, ax, ay * ay)) - __log2f(fmaf(ox, ox, oy * oy));
+    }
+  }
+  lj = warp_sum(lj);
+  mv.log_a = m * kLn2 * lj - 0.5f * (rn2 - r2) + log_qb - log_qf;
+  mv.jump2 = fmaf(c * dr - s * dt, c * dr - s * dt, (s * dr + c * dt) * (s * dr + c * dt));
+  return mv;
+}
+
+__device__ __forceinline__ void box_muller(uint32_t a, uint32_t b, float& e0, float& e1) {
+  const float rad = sqrtf(-2.f * __logf(u01(a)));
+  float sn, cs;
+  sincospif(2.f * u01(b), &sn, &cs);
+  e0 = rad * cs;
+  e1 = rad * sn;
+}
+
+__device__ void load_params(float* P, const __nv_bfloat16* w) {
+  for (int k = threadIdx.x; k < kNParams; k += blockDim.x) P[k] = __bfloat162float(w[k]);
+}
+
+__global__ void __launch_bounds__(kWarpsPerBlock * 32)
+learned_sweep_kernel(const SweepArgs a, const __nv_bfloat16* __restrict__ wts) {
+  __shared__ float P[kNParams];
+  extern __shared__ float2 zsm[];
+  load_params(P, wts);
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int w = blockIdx.x * kWarpsPerBlock + wib;
+  const bool live = w < a.W;
+  const int N = a.N;
+  float2* zs = zsm + size_t(wib) * N;
+  if (live)
+    for (int j = lane; j < N; j += 32) zs[j] = a.pos[size_t(w) * N + j];
+  __syncthreads();
+  if (!live) return;
+  __syncwarp();
+  const uint32_t sweep_base = a.sweep0 + (a.sweep_ctr ? *a.sweep_ctr : 0u);
+  const float m = float(a.m);
+  uint32_t nacc = 0;
+  for (int sw = 0; sw < a.n_sweeps; ++sw) {
+    const uint32_t sweep = sweep_base + uint32_t(sw);
+    for (int i = 0; i < N; ++i) {
+      const U4 r = philox4x32_10(U4{uint32_t(i), sweep, uint32_t(w), kTagLearned}, a.seed_lo, a.seed_hi);
+      float er, et;
+      box_muller(r.x, r.y, er, et);
+      const Move mv = propose(P, zs, N, i, a.invR, m, er, et, lane);
+      const bool acc = __logf(u01(r.z)) < mv.log_a;
+      __syncwarp();
+      if (acc) {
+        if (lane == (i & 31)) zs[i] = mv.zn;
+        ++nacc;
+      }
+      __syncwarp();
+    }
+  }
+  for (int j = lane; j < N; j += 32) a.pos[size_t(w) * N + j] = zs[j];
+  if (a.accepted && lane == 0) a.accepted[w] += nacc;
+  if (!a.measure) return;
+  // measurement record, the plain sweep's layout
+  float2 acc[kMaxDegree];
+#pragma unroll
+  for (int k = 0; k < kMaxDegree; ++k) acc[k] = make_float2(0.f, 0.f);
+  float h2 = 0.f, h4 = 0.f, hc[LEMC_MAX_PROBES], hs[LEMC_MAX_PROBES];
+#pragma unroll
+  for (int q = 0; q < LEMC_MAX_PROBES; ++q) hc[q] = hs[q] = 0.f;
+  for (int j = lane; j < N; j += 32) {
+    const float2 z = zs[j];
+    const float2 wv = make_float2(z.x * a.invR, z.y * a.invR);
+    float2 pw = wv;
+#pragma unroll
+    for (int k = 0; k < kMaxDegree; ++k) {
+      if (k < a.K) {
+        acc[k].x += pw.x;
+        acc[k].y += pw.y;
+        pw = make_float2(pw.x * wv.x - pw.y * wv.y, pw.x * wv.y + pw.y * wv.x);
+      }
+    }
+    const float r2 = fmaf(z.x, z.x, z.y * z.y);
+    h2 += r2;
+    h4 = fmaf(r2, r2, h4);
+    if (a.n_probes > 0) {
+      const float th = atan2f(z.y, z.x);
+#pragma unroll
+      for (int q = 0; q < LEMC_MAX_PROBES; ++q) {
+        if (q < a.n_probes) {
+          float sn, cs;
+          sincosf(float(a.probes[q]) * th, &sn, &cs);
+          hc[q] += cs;
+          hs[q] += sn;
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < kMaxDegree; ++k) {
+    if (k < a.K) {
+      acc[k].x = warp_sum(acc[k].x);
+      acc[k].y = warp_sum(acc[k].y);
+    }
+  }
+  h2 = warp_sum(h2);
+  h4 = warp_sum(h4);
+#pragma unroll
+  for (int q = 0; q < LEMC_MAX_PROBES; ++q) {
+    if (q < a.n_probes) {
+      hc[q] = warp_sum(hc[q]);
+      hs[q] = warp_sum(hs[q]);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < kMaxDegree; ++k)
+    if (k < a.K && (k & 31) == lane) a.rec_p[size_t(k) * a.W + w] = acc[k];
+  if (lane == 0) {
+    const size_t W = a.ldw;
+    a.rec_w[LEMC_W_ONE * W + w] = 1.f;
+    a.rec_w[LEMC_W_R2 * W + w] = h2;
+    a.rec_w[LEMC_W_R4 * W + w] = h4;
+    a.rec_w[LEMC_W_USER * W + w] = 0.f;
+#pragma unroll
+    for (int q = 0; q < LEMC_MAX_PROBES; ++q) {
+      if (q < a.n_probes) {
+        a.rec_w[(LEMC_W_PROBE0 + 2 * q) * W + w] = hc[q];
+        a.rec_w[(LEMC_W_PROBE0 + 2 * q + 1) * W + w] = hs[q];
+      }
+    }
+  }
+}
+
+// Network outputs and proposal densities for given (configuration, particle,
+// eps): out[s] = {mu_r, mu_t, log s_r, log s_t, z'.x, z'.y, ln A, |z'-z|^2}.
+__global__ void __launch_bounds__(kWarpsPerBlock * 32)
+learned_eval_kernel(const float2* __restrict__ cfgs, int n, int N, float invR, float m,
+                    const int32_t* __restrict__ particle, const float* __restrict__ eps,
+                    const __nv_bfloat16* __restrict__ wts, float* __restrict__ out) {
+  __shared__ float P[kNParams];
+  extern __shared__ float2 zsm[];
+  load_params(P, wts);
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int sidx = blockIdx.x * kWarpsPerBlock + wib;
+  float2* zs = zsm + size_t(wib) * N;
+  if (sidx < n)
+    for (int j = lane; j < N; j += 32) zs[j] = cfgs[size_t(sidx) * N + j];
+  __syncthreads();
+  if (sidx >= n) return;
+  __syncwarp();
+  const int i = particle[sidx];
+  const NetOut f = net_eval(P, zs, N, i, zs[i], invR, lane);
+  const Move mv = propose(P, zs, N, i, invR, m, eps[2 * sidx], eps[2 * sidx + 1], lane);
+  if (lane == 0) {
+    float* o = out + size_t(sidx) * 8;
+    o[0] = f.mr;
+    o[1] = f.mt;
+    o[2] = f.lr;
+    o[3] = f.lt;
+    o[4] = mv.zn.x;
+    o[5] = mv.zn.y;
+    o[6] = mv.log_a;
+    o[7] = mv.jump2;
+  }
+}
+
+// ES objective: block (x, pert) evaluates kWarpsPerBlock samples with the
+// parameters theta + sign * sigma * e_pair; J[pert] += sum of min(1, A) |dz|^2.
+__global__ void __launch_bounds__(kTrainWarps * 32)
+es_objective_kernel(const float2* __restrict__ cfgs, int n_cfg, int N, float invR, float m,
+                    const float* __restrict__ theta, float es_sigma, uint32_t step, uint32_t k0,
+                    uint32_t k1, int batch, double* __restrict__ J) {
+  __shared__ float P[kNParams];
+  __shared__ float part[kTrainWarps];
+  extern __shared__ float2 zsm[];
+  const int pert = blockIdx.y;
+  const int pair = pert >> 1;
+  const float sgn = (pert & 1) ? -es_sigma : es_sigma;
+  for (int k = threadIdx.x; k < kNParams; k += blockDim.x) {
+    const U4 r = philox4x32_10(U4{uint32_t(k), uint32_t(pair), step, kTagEs}, k0, k1);
+    float e0, e1;
+    box_muller(r.x, r.y, e0, e1);
+    P[k] = theta[k] + sgn * e0;
+  }
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int sidx = blockIdx.x * kTrainWarps + wib;
+  const bool live = sidx < batch;
+  const U4 r = philox4x32_10(U4{uint32_t(sidx), step, 0u, kTagTrain}, k0, k1);
+  const int c = int(r.x % uint32_t(n_cfg)), i = int(r.y % uint32_t(N));
+  float2* zs = zsm + size_t(wib) * N;
+  if (live)
+    for (int j = lane; j < N; j += 32) zs[j] = cfgs[size_t(c) * N + j];
+  __syncthreads();
+  float val = 0.f;
+  if (live) {
+    float er, et;
+    box_muller(r.z, r.w, er, et);
+    const Move mv = propose(P, zs, N, i, invR, m, er, et, lane);
+    val = (mv.log_a >= 0.f ? 1.f : __expf(mv.log_a)) * mv.jump2;
+    if (!(val == val)) val = 0.f;
+  }
+  if (lane == 0) part[wib] = val;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int q = 0; q < kTrainWarps; ++q) s += part[q];
+    atomicAdd(&J[pert], s);
+  }
+}
+
+// ES gradient (ascent on J) and one Adam step; the BF16 copy follows the
+// FP32 master weights.  trace[step] = mean J over all perturbations.
+__global__ void es_adam_kernel(float* __restrict__ theta, float* __restrict__ am,
+                               float* __restrict__ av, __nv_bfloat16* __restrict__ wts,
+                               const double* __restrict__ J, int pairs, int batch, float es_sigma,
+                               float lr, uint32_t step, uint32_t k0, uint32_t k1,
+                               double* __restrict__ trace) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k == 0) {
+    double s = 0.0;
+    for (int p = 0; p < 2 * pairs; ++p) s += J[p];
+    trace[step] = s / (2.0 * pairs * batch);
+  }
+  if (k >= kNParams) return;
+  double g = 0.0;
+  for (int p = 0; p < pairs; ++p) {
+    const U4 r = philox4x32_10(U4{uint32_t(k), uint32_t(p), step, kTagEs}, k0, k1);
+    float e0, e1;
+    box_muller(r.x, r.y, e0, e1);
+    g += (J[2 * p] - J[2 * p + 1]) * double(e0);
+  }
+  const float grad = float(g / (2.0 * pairs * batch * es_sigma));
+  const float b1 = 0.9f, b2 = 0.999f;
+  const float mk = b1 * am[k] + (1.f - b1) * grad;
+  const float vk = b2 * av[k] + (1.f - b2) * grad * grad;
+  am[k] = mk;
+  av[k] = vk;
+  const float t = float(step + 1);
+  const float mh = mk / (1.f - powf(b1, t)), vh = vk / (1.f - powf(b2, t));
+  const float th = theta[k] + lr * mh / (sqrtf(vh) + 1e-8f);
+  theta[k] = th;
+  wts[k] = __float2bfloat16_rn(th);
+}
+
+__global__ void to_bf16_kernel(const float* __restrict__ theta, __nv_bfloat16* __restrict__ wts) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < kNParams) wts[k] = __float2bfloat16_rn(theta[k]);
+}
+
+size_t walker_smem(int N, int warps = kWarpsPerBlock) { return size_t(warps) * N * sizeof(float2); }
+
+}  // namespace
+
+int launch_learned_sweep(const SweepArgs& a, const void* wts, cudaStream_t st) {
+  if (a.N > kMaxN || a.K > kMaxDegree) return LEMC_ERR_CAPACITY;
+  const int blocks = (a.W + kWarpsPerBlock - 1) / kWarpsPerBlock;
+  learned_sweep_kernel<<<blocks, kWarpsPerBlock * 32, walker_smem(a.N), st>>>(
+      a, static_cast<const __nv_bfloat16*>(wts));
+  return cudaPeekAtLastError() == cudaSuccess ? LEMC_OK : LEMC_ERR_CUDA;
+}
+
+}  // namespace lemc
+
+using namespace lemc;
+
+struct lemc_proposal {
+  int N = 0, m = 0;
+  float invR = 0.f;
+  float* theta = nullptr;       // FP32 master weights
+  float* am = nullptr;          // Adam moments
+  float* av = nullptr;
+  __nv_bfloat16* wts = nullptr; // BF16 weights the samplers read
+  double* J = nullptr;          // ES objective accumulators
+  int J_cap = 0;
+  double* trace = nullptr;
+  int trace_cap = 0;
+  uint64_t train_steps = 0;     // Adam steps taken (bias correction, Philox counters)
+};
+
+namespace {
+
+int upload_params(lemc_proposal* p, const float* host) {
+  if (cudaMemcpy(p->theta, host, sizeof(float) * kNParams, cudaMemcpyHostToDevice) != cudaSuccess)
+    return LEMC_ERR_CUDA;
+  to_bf16_kernel<<<(kNParams + 255) / 256, 256>>>(p->theta, p->wts);
+  if (cudaMemset(p->am, 0, sizeof(float) * kNParams) != cudaSuccess ||
+      cudaMemset(p->av, 0, sizeof(float) * kNParams) != cudaSuccess)
+    return LEMC_ERR_CUDA;
+  p->train_steps = 0;
+  return cudaDeviceSynchronize() == cudaSuccess ? LEMC_OK : LEMC_ERR_CUDA;
+}
+
+}  // namespace
+
+extern "C" int lemc_proposal_n_params(int* n) {
+  if (!n) return LEMC_ERR_ARG;
+  *n = kNParams;
+  return LEMC_OK;
+}
+
+extern "C" int lemc_proposal_create(int particles, int inverse_filling, float init_sigma,
+                                    uint64_t seed, lemc_proposal** out) {
+  if (!out) return LEMC_ERR_ARG;
+  *out = nullptr;
+  if (particles < 2 || inverse_filling < 1 || !(init_sigma > 0.f)) return LEMC_ERR_ARG;
+  if (particles > kMaxN) return LEMC_ERR_CAPACITY;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return LEMC_ERR_NODEVICE;
+  }
+  lemc_proposal* p = new lemc_proposal();
+  p->N = particles;
+  p->m = inverse_filling;
+  p->invR = float(1.0 / std::sqrt(2.0 * inverse_filling * particles));
+  bool ok = cudaMalloc(&p->theta, sizeof(float) * kNParams) == cudaSuccess &&
+            cudaMalloc(&p->am, sizeof(float) * kNParams) == cudaSuccess &&
+            cudaMalloc(&p->av, sizeof(float) * kNParams) == cudaSuccess &&
+            cudaMalloc(&p->wts, sizeof(__nv_bfloat16) * kNParams) == cudaSuccess;
+  if (!ok) {
+    lemc_proposal_destroy(p);
+    return LEMC_ERR_CUDA;
+  }
+  // start at the plain isotropic Gaussian step init_sigma: small random
+  // hidden weights, output weights near zero, output bias (0, 0, log s, log s)
+  std::mt19937_64 gen(seed);
+  std::normal_distribution<float> nd(0.f, 1.f);
+  std::vector<float> h(kNParams, 0.f);
+  for (int k = kOffW1; k < kOffB1; ++k) h[k] = 0.7f * nd(gen);
+  for (int k = kOffW2; k < kOffB2; ++k) h[k] = nd(gen) / std::sqrt(float(kIn));
+  for (int k = kOffW3; k < kOffB3; ++k) h[k] = 1e-3f * nd(gen);
+  h[kOffB3 + 2] = h[kOffB3 + 3] = std::log(init_sigma);
+  const int st = upload_params(p, h.data());
+  if (st != LEMC_OK) {
+    lemc_proposal_destroy(p);
+    return st;
+  }
+  *out = p;
+  return LEMC_OK;
+}
+
+extern "C" int lemc_proposal_destroy(lemc_proposal* p) {
+  if (!p) return LEMC_OK;
+  cudaFree(p->theta);
+  cudaFree(p->am);
+  cudaFree(p->av);
+  cudaFree(p->wts);
+  cudaFree(p->J);
+  cudaFree(p->trace);
+  delete p;
+  return LEMC_OK;
+}
+
+extern "C" int lemc_proposal_get_params(const lemc_proposal* p, float* host, int n) {
+  if (!p || !host || n != kNParams) return LEMC_ERR_ARG;
+  return cudaMemcpy(host, p->theta, sizeof(float) * kNParams, cudaMemcpyDeviceToHost) == cudaSuccess
+             ? LEMC_OK
+             : LEMC_ERR_CUDA;
+}
+
+extern "C" int lemc_proposal_set_params(lemc_proposal* p, const float* host, int n) {
+  if (!p || !host || n != kNParams) return LEMC_ERR_ARG;
+  return upload_params(p, host);
+}
+
+extern "C" int lemc_proposal_eval(const lemc_proposal* p, const float* host_xy, int n,
+                                  const int32_t* particle, const float* eps, float* out) {
+  if (!p || !host_xy || !particle || !eps || !out || n <= 0) return LEMC_ERR_ARG;
+  for (int s = 0; s < n; ++s)
+    if (particle[s] < 0 || particle[s] >= p->N) return LEMC_ERR_ARG;
+  const int N = p->N;
+  float2* d_cfg = nullptr;
+  int32_t* d_i = nullptr;
+  float *d_e = nullptr, *d_o = nullptr;
+  int st = LEMC_OK;
+  auto ok = [&](cudaError_t e) {
+    if (e != cudaSuccess && st == LEMC_OK) st = LEMC_ERR_CUDA;
+  };
+  ok(cudaMalloc(&d_cfg, sizeof(float2) * size_t(n) * N));
+  ok(cudaMalloc(&d_i, sizeof(int32_t) * n));
+  ok(cudaMalloc(&d_e, sizeof(float) * 2 * n));
+  ok(cudaMalloc(&d_o, sizeof(float) * 8 * n));
+  if (st == LEMC_OK) {
+    ok(cudaMemcpy(d_cfg, host_xy, sizeof(float2) * size_t(n) * N, cudaMemcpyHostToDevice));
+    ok(cudaMemcpy(d_i, particle, sizeof(int32_t) * n, cudaMemcpyHostToDevice));
+    ok(cudaMemcpy(d_e, eps, sizeof(float) * 2 * n, cudaMemcpyHostToDevice));
+  }
+  if (st == LEMC_OK) {
+    learned_eval_kernel<<<(n + kWarpsPerBlock - 1) / kWarpsPerBlock, kWarpsPerBlock * 32,
+                          walker_smem(N)>>>(d_cfg, n, N, p->invR, float(p->m), d_i, d_e, p->wts,
+                                            d_o);
+    ok(cudaPeekAtLastError());
+    ok(cudaDeviceSynchronize());
+    ok(cudaMemcpy(out, d_o, sizeof(float) * 8 * n, cudaMemcpyDeviceToHost));
+  }
+  cudaFree(d_cfg);
+  cudaFree(d_i);
+  cudaFree(d_e);
+  cudaFree(d_o);
+  return st;
+}
+
+extern "C" int lemc_proposal_train(lemc_proposal* p, const void* configs, int n_cfg,
+                                   const lemc_train_config* tc, double* trace) {
+  if (!p || !configs || n_cfg < 1 || !tc) return LEMC_ERR_ARG;
+  if (tc->steps < 1 || tc->batch < 1 || tc->pairs < 1 || !(tc->lr > 0.f) || !(tc->es_sigma > 0.f))
+    return LEMC_ERR_ARG;
+  const int N = p->N;
+  if (walker_smem(N, kTrainWarps) > 48 * 1024 - sizeof(float) * kNParams) return LEMC_ERR_CAPACITY;
+  if (p->J_cap < 2 * tc->pairs) {
+    cudaFree(p->J);
+    p->J = nullptr;
+    if (cudaMalloc(&p->J, sizeof(double) * 2 * tc->pairs) != cudaSuccess) return LEMC_ERR_CUDA;
+    p->J_cap = 2 * tc->pairs;
+  }
+  if (p->trace_cap < tc->steps) {
+    cudaFree(p->trace);
+    p->trace = nullptr;
+    if (cudaMalloc(&p->trace, sizeof(double) * tc->steps) != cudaSuccess) return LEMC_ERR_CUDA;
+    p->trace_cap = tc->steps;
+  }
+  const uint32_t k0 = uint32_t(tc->seed), k1 = uint32_t(tc->seed >> 32);
+  const dim3 grid((tc->batch + kTrainWarps - 1) / kTrainWarps, 2 * tc->pairs);
+  for (int s = 0; s < tc->steps; ++s) {
+    const uint32_t step = uint32_t(p->train_steps);
+    if (cudaMemsetAsync(p->J, 0, sizeof(double) * 2 * tc->pairs) != cudaSuccess) return LEMC_ERR_CUDA;
+    es_objective_kernel<<<grid, kTrainWarps * 32, walker_smem(N, kTrainWarps)>>>(
+        static_cast<const float2*>(configs), n_cfg, N, p->invR, float(p->m), p->theta,
+        tc->es_sigma, step, k0, k1, tc->batch, p->J);
+    es_adam_kernel<<<(kNParams + 255) / 256, 256>>>(p->theta, p->am, p->av, p->wts, p->J,
+                                                    tc->pairs, tc->batch, tc->es_sigma, tc->lr,
+                                                    step, k0, k1, p->trace + s);
+    if (cudaPeekAtLastError() != cudaSuccess) return LEMC_ERR_CUDA;
+    ++p->train_steps;
+  }
+  if (cudaDeviceSynchronize() != cudaSuccess) return LEMC_ERR_CUDA;
+  if (trace &&
+      cudaMemcpy(trace, p->trace, sizeof(double) * tc->steps, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return LEMC_ERR_CUDA;
+  return LEMC_OK;
+}
+
+// Weights of a proposal for the samplers of lemc_ctx (device BF16 array).
+const void* lemc_proposal_weights(const lemc_proposal* p) { return p ? p->wts : nullptr; }
+int lemc_proposal_particles(const lemc_proposal* p) { return p ? p->N : 0; }
+int lemc_proposal_filling(const lemc_proposal* p) { return p ? p->m : 0; }

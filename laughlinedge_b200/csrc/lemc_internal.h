@@ -72,6 +72,9 @@ int launch_init_walkers(float2* pos, int W, int N, float radius, uint32_t seed_l
 int launch_basis(const float2* rec_p, int W, int K, int N, const BasisNode* prog,
                  int n_nodes, float* V, int ldv, double* series, const uint32_t* series_idx,
                  cudaStream_t st);
+// Learned-proposal sweep (one walker per warp) with BF16 network weights wts;
+// same arguments, records and error conventions as launch_sweep (Laughlin guide).
+int launch_learned_sweep(const SweepArgs& a, const void* wts, cudaStream_t st);
 // ctr[0] += 1, ctr[1] += 1: sweep and measurement counters of a replayed graph
 int launch_advance_counters(uint32_t* ctr, cudaStream_t st);
 
@@ -112,3 +115,9 @@ size_t gram_tc_smem_bytes(int mode);
 constexpr int kTcSlot = 128 * 96;  // doubles per partial slot
 
 }  // namespace lemc
+
+// Internal accessors of a learned proposal (csrc/learned.cu).
+const void* lemc_proposal_weights(const lemc_proposal* p);
+int lemc_proposal_particles(const lemc_proposal* p);
+int lemc_proposal_filling(const lemc_proposal* p);
+

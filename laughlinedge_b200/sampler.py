@@ -249,6 +249,17 @@ class Sampler:
         check(self.lib.lemc_read_stats(self._h, C.byref(st)), "lemc_read_stats")
         return st
 
+    def set_proposal(self, proposal):
+        """Use a LearnedProposal for the sweeps (None: the plain Gaussian step)."""
+        check(self.lib.lemc_set_proposal(self._h, proposal._h if proposal is not None else None),
+              "lemc_set_proposal")
+        self._proposal = proposal  # keep the weights alive while in use
+
+    def copy_positions_device(self, dst_ptr: int):
+        """Device-to-device copy of the walker positions ([W][N] float2)."""
+        check(self.lib.lemc_copy_positions_device(self._h, C.c_void_p(dst_ptr)),
+              "lemc_copy_positions_device")
+
     def positions(self) -> np.ndarray:
         W, N = self.cfg.n_walkers, self.cfg.particles
         out = np.zeros(W * N * 2, dtype=np.float32)
