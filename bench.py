@@ -348,6 +348,105 @@ def run_ours(args, ws, rank, local):
     print(json.dumps(line), flush=True)
 
 
+LEARNED = {
+    "workload": "learned_proposal_m3_N200",
+    "particles": 200, "inverse_filling": 3, "omega": 1e-3, "kappa": 5e-6,
+    "sigma": 0.3, "walkers": 65536, "tau_walkers": 8192, "seed": 42,
+    "train_configs": 1 << 20, "train_steps": 5000, "train_batch": 1024, "train_pairs": 32,
+}
+
+
+def run_learned(args, rank, local):
+    """Learned vs plain single-particle proposal at equal sigma (N=200, m=3).
+
+    One line: walker-sweeps/s of each sampler (sweep kernel only, W=65536,
+    CUDA events), tau_int of p_1..p_4 of each (W=8192 chains, 1500 measured
+    sweeps after burn-in), effective samples/s = walker-sweeps/s / tau_int,
+    acceptance, and the training cost (5000 ES+Adam steps on 2^20
+    configurations drawn from the plain sampler)."""
+    if rank != 0:
+        return
+    import numpy as np
+    import torch
+
+    import laughlinedge_b200 as L
+    w = LEARNED
+    torch.cuda.set_device(local)
+    N, m, W = w["particles"], w["inverse_filling"], w["walkers"]
+    sectors = [1, 2, 3, 4]
+
+    def timed_sweeps(smp, n):
+        st = torch.cuda.ExternalStream(smp.stream())
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        smp.synchronize()
+        a.record(st)
+        smp.run(n, measure=False)
+        b.record(st)
+        b.synchronize()
+        return a.elapsed_time(b) / 1e3
+
+    # training data: snapshots of the plain chain
+    plain = L.Sampler(L.SamplerConfig(N, m, W, step_sigma=w["sigma"], seed=w["seed"],
+                                      lanes_per_walker=-1), sectors)
+    plain.init_walkers()
+    plain.run(args.burn + 100, measure=False)
+    n_snap = w["train_configs"] // W
+    cfg = torch.empty((n_snap * W, N, 2), dtype=torch.float32, device="cuda")
+    for k in range(n_snap):
+        plain.run(10, measure=False)
+        plain.copy_positions_device(cfg[k * W:(k + 1) * W].data_ptr())
+    plain.synchronize()
+    t_plain = timed_sweeps(plain, 20) / 20
+    plain.close()
+
+    prop = L.LearnedProposal(N, m, init_sigma=w["sigma"], seed=w["seed"])
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    trace = prop.train(cfg.data_ptr(), cfg.shape[0], steps=w["train_steps"], batch=w["train_batch"],
+                       pairs=w["train_pairs"], lr=3e-3, es_sigma=0.02, seed=w["seed"])
+    t_train = time.perf_counter() - t0
+    del cfg
+
+    lsmp = L.Sampler(L.SamplerConfig(N, m, W, step_sigma=w["sigma"], seed=w["seed"] + 1), sectors)
+    lsmp.set_proposal(prop)
+    lsmp.init_walkers()
+    lsmp.run(50, measure=False)
+    t_learned = timed_sweeps(lsmp, 5) / 5
+    lsmp.close()
+
+    def tau_run(use_prop):
+        smp = L.Sampler(L.SamplerConfig(N, m, w["tau_walkers"], step_sigma=w["sigma"],
+                                        seed=w["seed"] + 7, lanes_per_walker=0), sectors)
+        if use_prop:
+            smp.set_proposal(prop)
+        smp.init_walkers()
+        smp.run(args.burn + 400, measure=False)
+        smp.run(1500, measure=True)
+        st = smp.stats()
+        out = {"tau_int": st.tau_int, "tau_int_each": list(st.tau_int_each),
+               "acceptance": st.acceptance}
+        smp.close()
+        return out
+
+    tp, tl = tau_run(False), tau_run(True)
+    res = {}
+    for name, t, tau in (("plain", t_plain, tp), ("learned", t_learned, tl)):
+        ws_s = W / t
+        res[name] = dict(tau, walker_sweeps_per_s=ws_s, ms_per_sweep=1e3 * t,
+                         effective_samples_per_s=ws_s / tau["tau_int"])
+    line = {"metric": "effective_samples_per_s", "workload": w["workload"], "n_gpus": 1,
+            "unit": "samples/s", "higher_is_better": True, "data": "synthetic",
+            "config": {k: w[k] for k in w if k != "workload"},
+            "plain": res["plain"], "learned": res["learned"],
+            "learned_over_plain": res["learned"]["effective_samples_per_s"] /
+            res["plain"]["effective_samples_per_s"],
+            "tau_ratio_plain_over_learned": tp["tau_int"] / tl["tau_int"],
+            "train_seconds": t_train,
+            "train_objective_first_last": [float(np.mean(trace[:50])), float(np.mean(trace[-50:]))]}
+    prop.close()
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -357,6 +456,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--gram", default=None, choices=["fp64", "bf16x3", "bf16x4", "tf32x3"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--learned", action="store_true",
+                    help="learned vs plain proposal at N=200 (its own JSON line)")
     ap.add_argument("--graph-batch", type=int, default=32,
                     help="measured sweeps per CUDA-graph replay in the timed run (0: direct launches)")
     args = ap.parse_args()
@@ -364,7 +465,9 @@ def main():
         args.warmup = 3
     ws, rank, local = dist_init()
     try:
-        if args.impl == "reference":
+        if args.learned:
+            run_learned(args, rank, local)
+        elif args.impl == "reference":
             run_reference(args, ws, rank)
         else:
             run_ours(args, ws, rank, local)
