@@ -447,6 +447,74 @@ def run_learned(args, rank, local):
     print(json.dumps(line), flush=True)
 
 
+BATCHED = {
+    "workload": "batched_m3_N100_dL1-20_W131072",
+    "particles": 100, "inverse_filling": 3, "omega": 2e-3, "sectors": list(range(1, 21)),
+    "kappas": "16 log-spaced in [1e-6, 1e-4]", "walkers": 131072, "sigma": 0.3, "seed": 42,
+    "gram_mode": "tf32x3", "graph_batch": 8,
+}
+
+
+def run_batched(args, rank, local):
+    """Batched form: all 20 sectors (2713 states) and 16 quartic strengths.
+
+    Timed region: `steps` measured sweeps (sweep, basis, TF32x3 contraction
+    of S, H2, H4 for every sector) as CUDA-graph replays, CUDA events.  Then
+    the FP64 GPU tail solves every sector for the 16 strengths
+    (lemc_geneig_sweep), timed on the host clock."""
+    if rank != 0:
+        return
+    import numpy as np
+    import torch
+
+    import laughlinedge_b200 as L
+    w = BATCHED
+    torch.cuda.set_device(local)
+    N, m, W = w["particles"], w["inverse_filling"], w["walkers"]
+    steps = max(8, min(args.steps, 64))
+    steps -= steps % w["graph_batch"]
+    smp = L.Sampler(L.SamplerConfig(N, m, W, step_sigma=w["sigma"], seed=w["seed"],
+                                    lanes_per_walker=-1, gram_mode=L._lib.GRAM_TF32X3,
+                                    graph_batch=w["graph_batch"]), w["sectors"])
+    smp.init_walkers()
+    smp.run(args.burn, measure=False)
+    smp.run(max(args.warmup, w["graph_batch"]), measure=True)
+    smp.reset()
+    st_ = torch.cuda.ExternalStream(smp.stream())
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    smp.synchronize()
+    clk = Clocks(local)
+    a.record(st_)
+    smp.run(steps, measure=True)
+    b.record(st_)
+    b.synchronize()
+    clocks = clk.stop()
+    ms = a.elapsed_time(b) / steps
+    sd2, D = sum_d2(w["sectors"], N)
+    grams = [smp.gram(s)[:3] for s in range(len(w["sectors"]))]
+    acc = smp.stats().acceptance
+    G = smp.lanes_per_walker()
+    smp.close()
+    kap = np.logspace(-6, -4, 16)
+    t0 = time.perf_counter()
+    lowest = []
+    for S, H2, H4 in grams:
+        ev, _ = L.geneig_sweep(S, H2, H4, np.full(16, w["omega"]), kap, eps=1e-10)
+        lowest.append(float(ev[0, 0]))
+    t_tail = time.perf_counter() - t0
+    sh = W * sd2 * 3 / (ms * 1e-3)
+    line = {"metric": "sh_updates_per_s", "value": sh, "unit": "updates/s", "workload": w["workload"],
+            "n_gpus": 1, "steps": steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "dtype": "f32+tf32x3", "data": "synthetic",
+            "config": dict({k: w[k] for k in w if k not in ("workload", "sectors")},
+                           basis_states=D, sum_d2=sd2, lanes_per_walker=G),
+            "walker_sweeps_per_s": W / (ms * 1e-3), "acceptance": acc,
+            "contraction_tflops_algorithmic": W * 8.0 * 3 * sd2 / (ms * 1e-3) / 1e12,
+            "kappa_sweep_tail_s": t_tail, "kappa_sweep_problems": 16 * len(grams),
+            "lowest_level_per_sector_kappa0": lowest, "clocks": clocks}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -456,6 +524,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--gram", default=None, choices=["fp64", "bf16x3", "bf16x4", "tf32x3"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batched", action="store_true",
+                    help="batched form N=100, dL 1..20, 16 kappas (its own JSON line)")
     ap.add_argument("--learned", action="store_true",
                     help="learned vs plain proposal at N=200 (its own JSON line)")
     ap.add_argument("--graph-batch", type=int, default=32,
@@ -467,6 +537,8 @@ def main():
     try:
         if args.learned:
             run_learned(args, rank, local)
+        elif args.batched:
+            run_batched(args, rank, local)
         elif args.impl == "reference":
             run_reference(args, ws, rank)
         else:
