@@ -384,6 +384,19 @@ LEMC_API int lemc_evolve(int D, const double* M, const double* H, const double* 
                 double end_time, double save_step, double* out, double* norms,
                 int* n_save);
 
+/* The same evolution on the GPU in FP64, in the S-orthonormal basis of the
+ * canonical orthogonalisation of M (directions with metric eigenvalue <=
+ * eps * max dropped; *rank = kept dimension): C = X y, dy/dt = -i (X^H H X
+ * + f(t) X^H U X) y with the trace mean of X^H H X removed as a global phase,
+ * classical RK4 with step save_step / substeps.  f is evaluated on the host at
+ * every stage time before the integration starts.  Outputs as lemc_evolve.
+ * Replaces the host integration of timeEvolution::edgeDensityResponse_compute
+ * (modules/dynamics/dynamics.cpp:149-308) for fixed-step propagation. */
+LEMC_API int lemc_evolve_device(int D, const double* M, const double* H, const double* U,
+                                int L, const double* rho, lemc_profile_fn f, void* user,
+                                double end_time, double save_step, int substeps, double eps,
+                                double* out, double* norms, int* n_save, int* rank);
+
 #ifdef __cplusplus
 }
 #endif

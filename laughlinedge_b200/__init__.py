@@ -6,8 +6,8 @@ sm_100a behind the C-ABI of include/lemc.h); this package only binds it.
 from . import _lib
 from ._lib import LemcError, load
 from .proposal import LearnedProposal
-from .sampler import (Sampler, SamplerConfig, evolve, geneig, geneig_sweep, normalise,
+from .sampler import (Sampler, SamplerConfig, evolve, evolve_device, geneig, geneig_sweep, normalise,
                       partitions)
 
-__all__ = ["LearnedProposal", "LemcError", "Sampler", "SamplerConfig", "evolve", "geneig", "geneig_sweep", "load",
+__all__ = ["LearnedProposal", "LemcError", "Sampler", "SamplerConfig", "evolve", "evolve_device", "geneig", "geneig_sweep", "load",
            "normalise", "partitions", "_lib"]

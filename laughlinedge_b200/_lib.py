@@ -122,6 +122,8 @@ _SIGNATURES = {
     "lemc_geneig_sweep": ([_I, _DP, _DP, _DP, _DP, _DP, _I, _D, _DP, _IP], _I),
     "lemc_normalise": ([_I, _DP, _DP, _DP, _D, _D, _DP, _DP], _I),
     "lemc_evolve": ([_I, _DP, _DP, _DP, _I, _DP, PROFILE_FN, _P, _D, _D, _DP, _DP, _IP], _I),
+    "lemc_evolve_device": ([_I, _DP, _DP, _DP, _I, _DP, PROFILE_FN, _P, _D, _D, _I, _D, _DP, _DP,
+                            _IP, _IP], _I),
 }
 
 _lib = None

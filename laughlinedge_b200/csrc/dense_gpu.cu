@@ -174,3 +174,263 @@ extern "C" int lemc_geneig_sweep(int D, const double* S, const double* H2, const
   }
   return cudaDeviceSynchronize() == cudaSuccess ? LEMC_OK : LEMC_ERR_CUDA;
 }
+
+// ---- time evolution in the S-orthonormal basis ------------------------------
+// Reference: timeEvolution::edgeDensityResponse_compute (modules/dynamics/
+// dynamics.cpp:24-53, :149-308) integrates M dC/dt = -i (H + f(t) U) C on the
+// host with an adaptive Cash-Karp pair.  Here, on the GPU in FP64: with the
+// canonical orthogonalisation X of M (X^H M X = 1), C = X y and
+//   dy/dt = -i (H' + f(t) U') y,   H' = X^H H X - e I,  U' = X^H U X,
+// e = tr(H')/r removed as a global phase (no observable depends on it, and it
+// keeps h |H'| small).  Classical RK4 with h = save_step / substeps; every
+// stage is one fused kernel (axpy + the two matrix-vector products, one warp
+// per row).  Observables C^H rho_l C = y^H (X^H rho_l X) y and C^H M C = y^H y
+// are recorded on the device at every save point.
+namespace lemc {
+namespace {
+
+// row-major complex input -> column-major device layout (a transpose)
+__global__ void to_colmajor_kernel(int D, const double2* __restrict__ in, double2* __restrict__ out) {
+  const int i = blockIdx.y * blockDim.y + threadIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < D && j < D) out[size_t(j) * D + i] = in[size_t(i) * D + j];
+}
+
+// column-major r x r -> row-major, minus e on the diagonal
+__global__ void to_rowmajor_shift_kernel(int r, const double2* __restrict__ in, double e,
+                                         double2* __restrict__ out) {
+  const int i = blockIdx.y * blockDim.y + threadIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < r && j < r) {
+    double2 v = in[size_t(j) * r + i];
+    if (i == j) v.x -= e;
+    out[size_t(i) * r + j] = v;
+  }
+}
+
+__global__ void diag_mean_kernel(int r, const double2* __restrict__ A, double* __restrict__ out) {
+  __shared__ double s[256];
+  double v = 0.0;
+  for (int i = threadIdx.x; i < r; i += blockDim.x) v += A[size_t(i) * r + i].x;
+  s[threadIdx.x] = v;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) s[threadIdx.x] += s[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = s[0] / r;
+}
+
+__device__ __forceinline__ double2 cfma(double2 a, double2 b, double2 c) {
+  return make_double2(fma(a.x, b.x, fma(-a.y, b.y, c.x)), fma(a.x, b.y, fma(a.y, b.x, c.y)));
+}
+
+// k_out = -i (H + f U) (y + a k_in), one warp per row; rows row-major.
+__global__ void rk_stage_kernel(int r, const double2* __restrict__ Hr, const double2* __restrict__ Ur,
+                                const double2* __restrict__ y, const double2* __restrict__ kin,
+                                double a, double f, double2* __restrict__ kout) {
+  const int row = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (row >= r) return;
+  double2 sh = make_double2(0.0, 0.0), su = make_double2(0.0, 0.0);
+  for (int j = lane; j < r; j += 32) {
+    double2 v = y[j];
+    if (kin) v = make_double2(fma(a, kin[j].x, v.x), fma(a, kin[j].y, v.y));
+    sh = cfma(Hr[size_t(row) * r + j], v, sh);
+    su = cfma(Ur[size_t(row) * r + j], v, su);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    sh.x += __shfl_xor_sync(0xffffffffu, sh.x, o);
+    sh.y += __shfl_xor_sync(0xffffffffu, sh.y, o);
+    su.x += __shfl_xor_sync(0xffffffffu, su.x, o);
+    su.y += __shfl_xor_sync(0xffffffffu, su.y, o);
+  }
+  if (lane == 0) {
+    const double2 t = make_double2(sh.x + f * su.x, sh.y + f * su.y);
+    kout[row] = make_double2(t.y, -t.x);  // -i t
+  }
+}
+
+__global__ void rk_update_kernel(int r, double h, double2* __restrict__ y, const double2* __restrict__ k1,
+                                 const double2* __restrict__ k2, const double2* __restrict__ k3,
+                                 const double2* __restrict__ k4) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= r) return;
+  const double c = h / 6.0;
+  y[i].x += c * (k1[i].x + 2.0 * k2[i].x + 2.0 * k3[i].x + k4[i].x);
+  y[i].y += c * (k1[i].y + 2.0 * k2[i].y + 2.0 * k3[i].y + k4[i].y);
+}
+
+// out[l] = y^H R_l y for the L row-major r x r matrices R, and nrm = y^H y;
+// one block per l (block L computes the norm).
+__global__ void observe_kernel(int r, int L, const double2* __restrict__ R, const double2* __restrict__ y,
+                               double2* __restrict__ out, double* __restrict__ nrm) {
+  __shared__ double2 red[256];
+  const int l = blockIdx.x;
+  double2 acc = make_double2(0.0, 0.0);
+  if (l < L) {
+    const double2* A = R + size_t(l) * r * r;
+    for (int i = threadIdx.x; i < r; i += blockDim.x) {
+      double2 row = make_double2(0.0, 0.0);
+      for (int j = 0; j < r; ++j) row = cfma(A[size_t(i) * r + j], y[j], row);
+      const double2 yc = make_double2(y[i].x, -y[i].y);
+      acc = cfma(yc, row, acc);
+    }
+  } else {
+    for (int i = threadIdx.x; i < r; i += blockDim.x) acc.x += y[i].x * y[i].x + y[i].y * y[i].y;
+  }
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      red[threadIdx.x].x += red[threadIdx.x + o].x;
+      red[threadIdx.x].y += red[threadIdx.x + o].y;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    if (l < L) out[l] = red[0];
+    else *nrm = red[0].x;
+  }
+}
+
+}  // namespace
+}  // namespace lemc
+
+extern "C" int lemc_evolve_device(int D, const double* M, const double* H, const double* U, int L,
+                                  const double* rho, lemc_profile_fn f, void* user,
+                                  double end_time, double save_step, int substeps, double eps,
+                                  double* out, double* norms, int* n_save, int* rank) {
+  if (D <= 0 || !M || !H || !U || L < 0 || (L > 0 && !rho) || !(save_step > 0) ||
+      !(end_time > 0) || substeps < 1 || !(eps >= 0.0))
+    return LEMC_ERR_ARG;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return LEMC_ERR_NODEVICE;
+  }
+  const int ns = int(std::ceil(end_time / save_step));
+  if (n_save) *n_save = ns;
+  Gpu g;
+  if (cusolverDnCreate(&g.sol) != CUSOLVER_STATUS_SUCCESS) return LEMC_ERR_CUDA;
+  if (cublasCreate(&g.blas) != CUBLAS_STATUS_SUCCESS) return LEMC_ERR_CUDA;
+  const size_t DD = size_t(D) * D;
+  const int NM = 3 + L;  // M, H, U, rho_0..rho_{L-1}
+  double2* raw = g.alloc<double2>(DD);
+  double2* cm = g.alloc<double2>(DD * NM);  // column-major copies
+  double2* X = g.alloc<double2>(DD);
+  double2* T = g.alloc<double2>(DD);
+  double2* P = g.alloc<double2>(DD);
+  double* w = g.alloc<double>(D);
+  int* info = g.alloc<int>(1);
+  if (!raw || !cm || !X || !T || !P || !w || !info) return LEMC_ERR_CUDA;
+  const dim3 tb(16, 16), gb((D + 15) / 16, (D + 15) / 16);
+  for (int q = 0; q < NM; ++q) {
+    const double* src = q == 0 ? M : q == 1 ? H : q == 2 ? U : rho + size_t(2) * DD * (q - 3);
+    if (cudaMemcpy(raw, src, DD * sizeof(double2), cudaMemcpyHostToDevice) != cudaSuccess)
+      return LEMC_ERR_CUDA;
+    to_colmajor_kernel<<<gb, tb>>>(D, raw, cm + DD * q);
+  }
+  // canonical orthogonalisation of M (column-major copy 0 is overwritten by U)
+  if (cudaMemcpy(P, cm, DD * sizeof(double2), cudaMemcpyDeviceToDevice) != cudaSuccess)
+    return LEMC_ERR_CUDA;
+  int lwork = 0;
+  if (cusolverDnZheevd_bufferSize(g.sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, D,
+                                  reinterpret_cast<cuDoubleComplex*>(P), D, w, &lwork) !=
+      CUSOLVER_STATUS_SUCCESS)
+    return LEMC_ERR_CUDA;
+  double2* work = g.alloc<double2>(size_t(std::max(1, lwork)));
+  if (!work) return LEMC_ERR_CUDA;
+  if (cusolverDnZheevd(g.sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, D,
+                       reinterpret_cast<cuDoubleComplex*>(P), D, w,
+                       reinterpret_cast<cuDoubleComplex*>(work), lwork, info) != CUSOLVER_STATUS_SUCCESS)
+    return LEMC_ERR_CUDA;
+  std::vector<double> m(D);
+  int h_info = 0;
+  if (cudaMemcpy(m.data(), w, D * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy(&h_info, info, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return LEMC_ERR_CUDA;
+  if (h_info != 0 || !(m[D - 1] > 0.0)) return LEMC_ERR_NUMERIC;
+  int first = 0;
+  while (first < D && !(m[first] > eps * m[D - 1])) ++first;
+  const int r = D - first;
+  if (rank) *rank = r;
+  scale_columns_kernel<<<dim3((D + 127) / 128, r), 128>>>(D, r, first, P, w, X);
+  // projected matrices, row-major on the device: H', U', rho'_l
+  const size_t RR = size_t(r) * r;
+  double2* Hr = g.alloc<double2>(RR);
+  double2* Ur = g.alloc<double2>(RR);
+  double2* Rr = g.alloc<double2>(RR * std::max(1, L));
+  double2* A = g.alloc<double2>(RR);
+  double* emean = g.alloc<double>(1);
+  double2 *y = g.alloc<double2>(r), *k1 = g.alloc<double2>(r), *k2 = g.alloc<double2>(r),
+          *k3 = g.alloc<double2>(r), *k4 = g.alloc<double2>(r);
+  double2* obs = g.alloc<double2>(size_t(ns) * std::max(1, L));
+  double* nrm = g.alloc<double>(ns);
+  if (!Hr || !Ur || !Rr || !A || !emean || !y || !k1 || !k2 || !k3 || !k4 || !obs || !nrm)
+    return LEMC_ERR_CUDA;
+  const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0);
+  auto project = [&](const double2* Bcm) -> bool {  // A = X^H B X (column-major r x r)
+    return cublasZgemm(g.blas, CUBLAS_OP_N, CUBLAS_OP_N, D, r, D, &one,
+                       reinterpret_cast<const cuDoubleComplex*>(Bcm), D,
+                       reinterpret_cast<const cuDoubleComplex*>(X), D, &zero,
+                       reinterpret_cast<cuDoubleComplex*>(T), D) == CUBLAS_STATUS_SUCCESS &&
+           cublasZgemm(g.blas, CUBLAS_OP_C, CUBLAS_OP_N, r, r, D, &one,
+                       reinterpret_cast<const cuDoubleComplex*>(X), D,
+                       reinterpret_cast<const cuDoubleComplex*>(T), D, &zero,
+                       reinterpret_cast<cuDoubleComplex*>(A), r) == CUBLAS_STATUS_SUCCESS;
+  };
+  const dim3 gr((r + 15) / 16, (r + 15) / 16);
+  if (!project(cm + DD)) return LEMC_ERR_CUDA;
+  diag_mean_kernel<<<1, 256>>>(r, A, emean);
+  double e = 0.0;
+  if (cudaMemcpy(&e, emean, sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess) return LEMC_ERR_CUDA;
+  to_rowmajor_shift_kernel<<<gr, tb>>>(r, A, e, Hr);
+  if (!project(cm + 2 * DD)) return LEMC_ERR_CUDA;
+  to_rowmajor_shift_kernel<<<gr, tb>>>(r, A, 0.0, Ur);
+  for (int l = 0; l < L; ++l) {
+    if (!project(cm + DD * (3 + l))) return LEMC_ERR_CUDA;
+    to_rowmajor_shift_kernel<<<gr, tb>>>(r, A, 0.0, Rr + RR * l);
+  }
+  // y(0) = X^H M e_0 (C(0) = e_0)
+  if (cublasZgemv(g.blas, CUBLAS_OP_C, D, r, &one, reinterpret_cast<const cuDoubleComplex*>(X), D,
+                  reinterpret_cast<const cuDoubleComplex*>(cm), 1, &zero,
+                  reinterpret_cast<cuDoubleComplex*>(y), 1) != CUBLAS_STATUS_SUCCESS)
+    return LEMC_ERR_CUDA;
+  if (cudaPeekAtLastError() != cudaSuccess) return LEMC_ERR_CUDA;
+  // profile values at every stage time, evaluated on the host
+  const double h = save_step / substeps;
+  const size_t nsteps = size_t(ns > 1 ? ns - 1 : 0) * substeps;
+  std::vector<double> fv(3 * nsteps);
+  for (size_t k = 0; k < nsteps; ++k) {
+    const double t = double(k) * h;
+    fv[3 * k] = f ? f(t, user) : 0.0;
+    fv[3 * k + 1] = f ? f(t + 0.5 * h, user) : 0.0;
+    fv[3 * k + 2] = f ? f(t + h, user) : 0.0;
+  }
+  const int wpb = 8, sblocks = (r + wpb - 1) / wpb, ublocks = (r + 255) / 256;
+  observe_kernel<<<L + 1, 256>>>(r, L, Rr, y, obs, nrm);
+  size_t k = 0;
+  for (int s = 1; s < ns; ++s) {
+    for (int q = 0; q < substeps; ++q, ++k) {
+      rk_stage_kernel<<<sblocks, 32 * wpb>>>(r, Hr, Ur, y, nullptr, 0.0, fv[3 * k], k1);
+      rk_stage_kernel<<<sblocks, 32 * wpb>>>(r, Hr, Ur, y, k1, 0.5 * h, fv[3 * k + 1], k2);
+      rk_stage_kernel<<<sblocks, 32 * wpb>>>(r, Hr, Ur, y, k2, 0.5 * h, fv[3 * k + 1], k3);
+      rk_stage_kernel<<<sblocks, 32 * wpb>>>(r, Hr, Ur, y, k3, h, fv[3 * k + 2], k4);
+      rk_update_kernel<<<ublocks, 256>>>(r, h, y, k1, k2, k3, k4);
+    }
+    observe_kernel<<<L + 1, 256>>>(r, L, Rr, y, obs + size_t(s) * std::max(1, L), nrm + s);
+  }
+  if (cudaPeekAtLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess)
+    return LEMC_ERR_CUDA;
+  if (L > 0 && out) {
+    std::vector<double2> all(size_t(ns) * L);
+    if (cudaMemcpy(all.data(), obs, all.size() * sizeof(double2), cudaMemcpyDeviceToHost) != cudaSuccess)
+      return LEMC_ERR_CUDA;
+    for (size_t q = 0; q < all.size(); ++q) {
+      out[2 * q] = all[q].x;
+      out[2 * q + 1] = all[q].y;
+    }
+  }
+  if (norms && cudaMemcpy(norms, nrm, ns * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return LEMC_ERR_CUDA;
+  return LEMC_OK;
+}

@@ -106,6 +106,27 @@ def evolve(M, H, U, rho, profile, end_time, save_step):
     return times, out.view(np.complex128).reshape(ns, max(L, 1))[:, :L], norms
 
 
+def evolve_device(M, H, U, rho, profile, end_time, save_step, substeps=4, eps=1e-12):
+    """Fixed-step FP64 GPU evolution in the S-orthonormal basis; returns
+    (times, <rho_l>(t) [n_save, L], norms, rank)."""
+    lib = _lib.load()
+    D = M.shape[0]
+    rho = [np.ascontiguousarray(r, dtype=np.complex128) for r in rho]
+    L = len(rho)
+    rb = np.ascontiguousarray(np.stack(rho) if L else np.zeros((1, D, D), complex)).view(np.float64).ravel()
+    ns = int(math.ceil(end_time / save_step))
+    out = np.zeros(2 * ns * max(L, 1))
+    norms = np.zeros(ns)
+    n_save, rank = C.c_int(), C.c_int()
+    cb = _lib.PROFILE_FN(lambda t, u: float(profile(t)))
+    a = [np.ascontiguousarray(X, dtype=np.complex128).view(np.float64).ravel() for X in (M, H, U)]
+    check(lib.lemc_evolve_device(D, dptr(a[0]), dptr(a[1]), dptr(a[2]), L, dptr(rb), cb, None,
+                                 end_time, save_step, substeps, eps, dptr(out), dptr(norms),
+                                 C.byref(n_save), C.byref(rank)), "lemc_evolve_device")
+    times = np.arange(ns) * save_step
+    return times, out.view(np.complex128).reshape(ns, max(L, 1))[:, :L], norms, rank.value
+
+
 def occupation(particles, inverse_filling, dL, l_cutoff, n_walkers, sweeps, burn_in=200,
                step_sigma=0.3, seed=42):
     """Occupation averages for every (L, R) row pair of sector dL: complex [D, D, l_cutoff]."""
