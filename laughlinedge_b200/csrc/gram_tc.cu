@@ -25,7 +25,7 @@
 // read it from there, so shared memory only carries the raw TMA stages and
 // the (weighted, split) B operand.
 //
-// Pipeline (576 threads, one CTA per SM):
+// Pipeline (608 threads, one CTA per SM):
 //   warp 17      loader: tiled TMA loads per K-chunk (A panel 128 x KC in
 //                128-byte-swizzled boxes of 32 samples, B panel 32 x KC,
 //                weight planes 3 x KC; rows past the end are zero-filled by
@@ -35,6 +35,8 @@
 //   warps 12-15  B converters: raw FP32 -> weighted, split hi/lo B operands in
 //                128-byte-swizzled K-major shared-memory layout;
 //   warp 16      allocates 512 TMEM columns, one lane issues tcgen05.mma;
+//   warp 18      scheduler: makes the issuer's barrier waits and hands each
+//                K-chunk to it through a named barrier;
 //   warps 0-7    epilogue: TMEM lane quarter = warp % 4, column half =
 //                warp / 4, 48 FP32 accumulators per thread.
 // Tensor memory columns: hi*hi buffers at 0 and 128, corrections at 256, A
@@ -65,7 +67,8 @@ constexpr int kConvThreads = 8 * 32;
 constexpr int kEpiCols = kN / (kEpiWarps / 4);  // accumulator columns per epilogue thread
 constexpr int kMmaWarp = 16;
 constexpr int kLoadWarp = 17;
-constexpr int kThreads = 18 * 32;
+constexpr int kSchedWarp = 18;     // does the issuer's barrier waits (see the MMA issuer)
+constexpr int kThreads = 19 * 32;
 constexpr int kTmemCols = 512;
 constexpr uint32_t kColHH = 0;     // hi*hi buffers at 0 and 128
 constexpr uint32_t kColCorr = 256; // corrections
@@ -116,6 +119,17 @@ __device__ __forceinline__ void mbar_arrive_tx(uint64_t* bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
                "r"(bytes)
                : "memory");
+}
+
+// CTA named barriers (0 is __syncthreads), 64 threads each: ids 1/2 hand
+// K-chunk c (by parity) from the scheduler warp to the MMA warp ("ready"),
+// ids 3/4 return it ("issued"), so neither warp can run two chunks ahead of
+// the other and every barrier completes with exactly 32 + 32 threads.
+__device__ __forceinline__ void named_arrive(int id) {
+  asm volatile("bar.arrive %0, 64;" ::"r"(id) : "memory");
+}
+__device__ __forceinline__ void named_sync(int id) {
+  asm volatile("bar.sync %0, 64;" ::"r"(id) : "memory");
 }
 
 __device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
@@ -470,27 +484,56 @@ gram_tc_kernel(const TcArgs a, const __grid_constant__ CUtensorMap tmA,
       mbar_arrive(&sm->op_full[os]);
       mbar_arrive(&sm->raw_empty[rs]);
     }
+  } else if (warp == kSchedWarp) {
+    // ------------------------------ scheduler -------------------------------
+    // An mbarrier test made by the thread that has just issued tcgen05.commit
+    // stalls until the committed MMAs retire, which drains the tensor pipe every
+    // K-chunk.  So this warp makes the issuer's waits (operand stage full;
+    // hi*hi buffer empty at the start of a flush group) and hands each chunk
+    // over through a named barrier, which needs no shared-memory access.  It
+    // arrives once per chunk whatever happens (after an abort without
+    // waiting), so the issuer's barrier always completes.
+    int s = 0, b = 0, f = 0;
+    uint32_t ph_op = 0, ph_acc = 0;
+    for (int c = 0; c < nch; ++c) {
+      if (c >= 2) named_sync(3 + (c & 1));  // chunk c-2 issued: ids 1/2 are free again
+      if (lane == 0 && !*(volatile int*)abort_flag) {
+        bool ok = true;
+        if (f == 0) {
+          ok = mbar_wait(&sm->acc_empty[b], ((ph_acc >> b) & 1u) ^ 1u, abort_flag, a.err);
+          ph_acc ^= 1u << b;
+        }
+        if (ok) mbar_wait(&sm->op_full[s], ph_op, abort_flag, a.err);
+      }
+      __syncwarp();
+      named_arrive(1 + (c & 1));
+      if (++f == F || c == nch - 1) {
+        f = 0;
+        b ^= 1;
+      }
+      if (++s == kOpStages) {
+        s = 0;
+        ph_op ^= 1u;
+      }
+    }
+    for (int c = max(0, nch - 2); c < nch; ++c) named_sync(3 + (c & 1));
   } else if (warp == kMmaWarp) {
     // ------------------------------ MMA issuer -----------------------------
     // One thread issues every MMA, so its per-MMA instruction count bounds the
     // tensor-core issue rate: all descriptors and TMEM addresses are formed
     // once per stage, a K step only adds a constant, and the flush schedule is
-    // tracked with counters instead of divisions.
-    if (lane == 0) {
-      const bool four = a.passes > 3;
-      static_assert(kOpStages == 2, "the issuer keeps one descriptor per operand stage");
-      const uint64_t bdesc0 = sw128_desc(smem_u32(sm->bop[0]));
-      const uint64_t bdesc1 = sw128_desc(smem_u32(sm->bop[1]));
-      constexpr uint64_t kLoDesc = uint64_t(kBTileBytes >> 4);  // B lo tile, in descriptor units
-      int s = 0, b = 0, f = 0;          // operand stage, hi*hi buffer, chunk within flush group
-      uint32_t ph_op = 0, ph_acc = 0;   // ph_acc bit b: phase of hi*hi buffer b
-      for (int c = 0; c < nch; ++c) {
-        if (f == 0) {
-          if (!mbar_wait(&sm->acc_empty[b], ((ph_acc >> b) & 1u) ^ 1u, abort_flag, a.err)) break;
-          ph_acc ^= 1u << b;
-          tc_fence_after();
-        }
-        if (!mbar_wait(&sm->op_full[s], ph_op, abort_flag, a.err)) break;
+    // kept in counters.  Its waits are made by the scheduler warp.
+    const bool four = a.passes > 3;
+    static_assert(kOpStages == 2, "the issuer keeps one descriptor per operand stage");
+    const uint64_t bdesc0 = sw128_desc(smem_u32(sm->bop[0]));
+    const uint64_t bdesc1 = sw128_desc(smem_u32(sm->bop[1]));
+    constexpr uint64_t kLoDesc = uint64_t(kBTileBytes >> 4);  // B lo tile, in descriptor units
+    int s = 0, b = 0, f = 0;          // operand stage, hi*hi buffer, chunk within flush group
+    int issued = 0;
+    for (int c = 0; c < nch; ++c) {
+      named_sync(1 + (c & 1));
+      const bool go = !*(volatile int*)abort_flag;
+      if (lane == 0 && go) {
         tc_fence_after();
         const uint64_t bh = s ? bdesc1 : bdesc0, bl = bh + kLoDesc;
         const uint32_t ahi = tmem + kColA + uint32_t(s * 64), alo = ahi + 32;
@@ -510,23 +553,22 @@ gram_tc_kernel(const TcArgs a, const __grid_constant__ CUtensorMap tmA,
           if (four) mma_ts<TF32>(dc, alo + 8 * ks, bl + 2 * ks, IDESC, 1u);
         }
         umma_commit(&sm->op_empty[s]);
-        const bool last = (c == nch - 1);
-        if (++f == F || last) {
-          umma_commit(&sm->acc_full[b]);
-          f = 0;
-          b ^= 1;
-        }
-        if (last) umma_commit(&sm->corr_full);
-        if (++s == kOpStages) {
-          s = 0;
-          ph_op ^= 1u;
-        }
+        if (f + 1 == F || c == nch - 1) umma_commit(&sm->acc_full[b]);
+        if (c == nch - 1) umma_commit(&sm->corr_full);
+        ++issued;
       }
-      if (nch > 0) {
-        // every issued MMA must retire before TMEM is released
-        umma_commit(&sm->done);
-        mbar_wait(&sm->done, 0u, abort_flag, a.err);
+      __syncwarp();
+      named_arrive(3 + (c & 1));
+      if (++f == F || c == nch - 1) {
+        f = 0;
+        b ^= 1;
       }
+      if (++s == kOpStages) s = 0;
+    }
+    if (lane == 0 && issued > 0) {
+      // every issued MMA must retire before TMEM is released
+      umma_commit(&sm->done);
+      mbar_wait(&sm->done, 0u, abort_flag, a.err);
     }
     __syncwarp();
   } else if (warp < kEpiWarps) {
