@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <string>
@@ -129,7 +130,8 @@ struct lemc_ctx {
   DevBuf<float> V;
   DevBuf<uint32_t> accepted;
   DevBuf<BasisNode> prog;
-  int n_nodes = 0;
+  DevBuf<int> prog_seg;
+  BasisProgram bprog;
   DevBuf<GramJob> jobs;
   DevBuf<double> gram;      // 3 planes x gram_plane complex
   DevBuf<double> cross;     // 3 planes x cross_plane complex
@@ -227,10 +229,43 @@ int build_program(lemc_ctx* c) {
   }
   // the DFS above extends sequences with parts <= previous part, i.e. each
   // multiset exactly once, ordered non-increasingly.
-  c->n_nodes = int(prog.size());
+  const int n = int(prog.size());
+  int max_depth = 0, max_part = 0;
+  for (const BasisNode& nd : prog) {
+    max_depth = std::max(max_depth, nd.depth);
+    max_part = std::max(max_part, nd.part);
+  }
+  prog.push_back({0, 0, -1, -1});  // two sentinels: the kernel reads up to two nodes ahead
+  prog.push_back({0, 0, -1, -1});
   LEMC_TRY(c->prog.alloc(prog.size()));
   LEMC_CUDA(cudaMemcpy(c->prog.p, prog.data(), prog.size() * sizeof(BasisNode),
                        cudaMemcpyHostToDevice));
+  // Segments: cut at the depth-1 node nearest to each of the kMaxBasisSegments
+  // equal shares of the program.
+  BasisProgram& bp = c->bprog;
+  bp = BasisProgram{};
+  bp.nodes = c->prog.p;
+  bp.n_nodes = n;
+  bp.max_depth = max_depth;
+  bp.max_part = max_part;
+  std::vector<int> roots;
+  for (int t = 1; t < n; ++t)
+    if (prog[t].depth == 1) roots.push_back(t);
+  std::vector<int> cuts{0};
+  for (int k = 1; k < kMaxBasisSegments; ++k) {
+    const long ideal = long(k) * n / kMaxBasisSegments;
+    int best = -1;
+    for (int r : roots)
+      if (r > cuts.back() && (best < 0 || std::labs(r - ideal) < std::labs(best - ideal))) best = r;
+    if (best > cuts.back()) cuts.push_back(best);
+  }
+  cuts.push_back(n);
+  bp.n_seg = int(cuts.size()) - 1;
+  for (int j = 0; j < bp.n_seg; ++j) bp.max_seg = std::max(bp.max_seg, cuts[j + 1] - cuts[j]);
+  LEMC_TRY(c->prog_seg.alloc(cuts.size()));
+  LEMC_CUDA(cudaMemcpy(c->prog_seg.p, cuts.data(), cuts.size() * sizeof(int),
+                       cudaMemcpyHostToDevice));
+  bp.seg_dev = c->prog_seg.p;
   return LEMC_OK;
 }
 
@@ -590,6 +625,7 @@ int lemc_destroy(lemc_ctx* c) {
   c->V.release();
   c->accepted.release();
   c->prog.release();
+  c->prog_seg.release();
   c->jobs.release();
   c->gram.release();
   c->cross.release();
@@ -814,7 +850,7 @@ static int graph_step(lemc_ctx* c) {
   a.sweep0 = 0;
   a.sweep_ctr = c->d_ctr.p;
   LEMC_TRY(launch_sweep_for(c, a));
-  LEMC_TRY(launch_basis(c->rec_p.p, c->W, c->K, c->N, c->prog.p, c->n_nodes, c->V.p, c->Wpad,
+  LEMC_TRY(launch_basis(c->rec_p.p, c->W, c->K, c->N, c->bprog, c->V.p, c->Wpad,
                         c->series.p, c->d_ctr.p + 1, c->stream));
   LEMC_TRY(gram_step(c, c->V.p, c->rec_w.p, c->Wpad, c->W, c->cfg.gram_mode));
   return launch_advance_counters(c->d_ctr.p, c->stream);
@@ -899,7 +935,7 @@ static int run_impl(lemc_ctx* c, int n_sweeps, int measure, lemc_step_hook hook,
     LEMC_TRY(sweep_once(c, 1, 1));
     c->sweeps += 1;
     if (c->profile) LEMC_CUDA(cudaEventRecord(c->pev[4 * s + 1], c->stream));
-    LEMC_TRY(launch_basis(c->rec_p.p, c->W, c->K, c->N, c->prog.p, c->n_nodes, c->V.p, c->Wpad,
+    LEMC_TRY(launch_basis(c->rec_p.p, c->W, c->K, c->N, c->bprog, c->V.p, c->Wpad,
                           c->series.p + 8 * size_t(s), nullptr, c->stream));
     if (hook) {
       if (!c->hooked) ++c->version;
@@ -1105,7 +1141,7 @@ int lemc_basis_device(lemc_ctx* c, const void* rec_p, int W, void* V, int ldv, v
   if (!c || !rec_p || !V || W <= 0 || ldv < W) return LEMC_ERR_ARG;
   if (!c->has_basis) return LEMC_ERR_STATE;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  LEMC_TRY(launch_basis(static_cast<const float2*>(rec_p), W, c->K, c->N, c->prog.p, c->n_nodes,
+  LEMC_TRY(launch_basis(static_cast<const float2*>(rec_p), W, c->K, c->N, c->bprog,
                         static_cast<float*>(V), ldv, nullptr, nullptr, st));
   return order_after(c, st);
 }

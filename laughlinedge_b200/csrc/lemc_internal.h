@@ -35,11 +35,25 @@ struct SweepArgs {
 
 // Node of the depth-first basis program: value[depth] = value[depth-1] * p_part
 // (part 0 stands for p_0 = N); rows < 0 mean "not an output".
-struct BasisNode {
+struct alignas(16) BasisNode {
   int depth;
   int part;
   int row_re;
   int row_im;
+};
+
+// The program on the device, cut at depth-1 nodes into segments that need
+// only value[0] = 1 and so run as independent thread blocks.  The device
+// array holds n_nodes nodes followed by two sentinels {0, 0, -1, -1}.
+constexpr int kMaxBasisSegments = 8;
+struct BasisProgram {
+  const BasisNode* nodes = nullptr;
+  int n_nodes = 0;
+  int max_depth = 0;
+  int max_part = 0;
+  int n_seg = 0;
+  int max_seg = 0;  // longest segment, in nodes
+  const int* seg_dev = nullptr;  // n_seg + 1 segment starts (node indices), on the device
 };
 
 // One tile of the SIMT FP64 Gram accumulation: three weighted sums
@@ -69,9 +83,8 @@ int launch_init_walkers(float2* pos, int W, int N, float radius, uint32_t seed_l
                         uint32_t seed_hi, cudaStream_t st);
 
 // series_idx (may be null): the walker-mean series goes to series + 8 * *series_idx
-int launch_basis(const float2* rec_p, int W, int K, int N, const BasisNode* prog,
-                 int n_nodes, float* V, int ldv, double* series, const uint32_t* series_idx,
-                 cudaStream_t st);
+int launch_basis(const float2* rec_p, int W, int K, int N, const BasisProgram& prog, float* V,
+                 int ldv, double* series, const uint32_t* series_idx, cudaStream_t st);
 // Learned-proposal sweep (one walker per warp) with BF16 network weights wts;
 // same arguments, records and error conventions as launch_sweep (Laughlin guide).
 int launch_learned_sweep(const SweepArgs& a, const void* wts, cudaStream_t st);

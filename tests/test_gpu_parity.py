@@ -90,9 +90,10 @@ def _sampler(lemc, **kw):
     return lemc.Sampler(cfg, kw["sectors"])
 
 
-def test_basis_and_fp64_gram_match_oracle(lemc, oracle, cuda_ctx):
+@pytest.mark.parametrize("W", [256, 201])  # paired-walker and single-walker basis kernels
+def test_basis_and_fp64_gram_match_oracle(lemc, oracle, cuda_ctx, W):
     torch = cuda_ctx
-    N, m, W, seed = 8, 3, 256, 11
+    N, m, seed = 8, 3, 11
     sectors = [0, 1, 2, 3, 4, 5, 6]
     R = math.sqrt(2 * m * N)
     smp = _sampler(lemc, particles=N, inverse_filling=m, n_walkers=W, sectors=sectors)
