@@ -30,6 +30,7 @@ namespace lemc {
 namespace {
 
 constexpr float kLog2e = 1.4426950408889634f;
+constexpr float kTiny = 0x1p-64f;  // added to every squared pair distance
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -106,6 +107,9 @@ sweep_kernel(const SweepArgs a) {
     }
   }
 
+  const int tfull = N / G;                 // slots that hold a particle in every lane
+  const bool trem = tfull * G < N;         // a partly filled slot tfull follows
+  const bool rem_lane = gl < N - tfull * G;  // ... and holds a particle in this lane
   const float sigma = a.sigma;
   const float invR = a.invR;
   const float mf = float(a.m);
@@ -157,28 +161,51 @@ sweep_kernel(const SweepArgs a) {
         const float yn = __shfl_sync(0xffffffffu, pzy, b, G);
         const float lu = __shfl_sync(0xffffffffu, plu, b, G);
 
-        // Jastrow log2-ratio over this lane's particles: two independent
-        // product chains, masked (not branched) for j == i and the padding,
-        // one log2 per chain every 16 slots keeps FP32 in range.
+        // Jastrow log2-ratio over this lane's particles j = gl + t G in two
+        // independent product chains, one log2 per chain every 16 slots
+        // (keeps FP32 in range).  No per-pair masks: every squared distance
+        // carries + 2^-64, which leaves any distance above 2^-40 unchanged and
+        // turns the self pair j == im into the factors (s + 2^-64) / 2^-64,
+        // removed once after the loop; the padding of the remainder slot is
+        // masked outside the loop.
         float part = 0.f;
-        for (int c0 = 0; c0 < T2; c0 += 16) {
-          float n0 = 1.f, d0 = 1.f, n1 = 1.f, d1 = 1.f;
-          const int cend = min(T2, c0 + 16);
-          for (int t = c0; t < cend; t += 2) {
-            const int ja = gl + t * G, jb = ja + G;
-            const float2 za = zs[ja], zb = zs[jb];
+        {
+          float n0 = 1.f, d0 = 1.f;
+          if (trem) {  // slot tfull holds particles only in lanes gl < N - tfull G
+            const float2 za = zs[gl + tfull * G];
             const float ax = xn - za.x, ay = yn - za.y, ex = zo.x - za.x, ey = zo.y - za.y;
-            const float bx = xn - zb.x, by = yn - zb.y, fx = zo.x - zb.x, fy = zo.y - zb.y;
-            const float pa = fmaf(ax, ax, ay * ay), qa = fmaf(ex, ex, ey * ey);
-            const float pb = fmaf(bx, bx, by * by), qb = fmaf(fx, fx, fy * fy);
-            const bool va = (ja < N) && (ja != im);
-            const bool vb = (jb < N) && (jb != im);
-            n0 *= va ? pa : 1.f;
-            d0 *= va ? qa : 1.f;
-            n1 *= vb ? pb : 1.f;
-            d1 *= vb ? qb : 1.f;
+            const float pa = fmaf(ax, ax, fmaf(ay, ay, kTiny));
+            const float qa = fmaf(ex, ex, fmaf(ey, ey, kTiny));
+            n0 = rem_lane ? pa : 1.f;
+            d0 = rem_lane ? qa : 1.f;
           }
-          part += (__log2f(n0) + __log2f(n1)) - (__log2f(d0) + __log2f(d1));
+          for (int c0 = 0; c0 < tfull || c0 == 0; c0 += 16) {
+            float n1 = 1.f, d1 = 1.f;
+            const int cend = min(tfull, c0 + 16);
+            int t = c0;
+            for (; t + 1 < cend; t += 2) {
+              const float2 za = zs[gl + t * G], zb = zs[gl + (t + 1) * G];
+              const float ax = xn - za.x, ay = yn - za.y, ex = zo.x - za.x, ey = zo.y - za.y;
+              const float bx = xn - zb.x, by = yn - zb.y, fx = zo.x - zb.x, fy = zo.y - zb.y;
+              n0 *= fmaf(ax, ax, fmaf(ay, ay, kTiny));
+              d0 *= fmaf(ex, ex, fmaf(ey, ey, kTiny));
+              n1 *= fmaf(bx, bx, fmaf(by, by, kTiny));
+              d1 *= fmaf(fx, fx, fmaf(fy, fy, kTiny));
+            }
+            if (t < cend) {
+              const float2 za = zs[gl + t * G];
+              const float ax = xn - za.x, ay = yn - za.y, ex = zo.x - za.x, ey = zo.y - za.y;
+              n1 *= fmaf(ax, ax, fmaf(ay, ay, kTiny));
+              d1 *= fmaf(ex, ex, fmaf(ey, ey, kTiny));
+            }
+            part += (__log2f(n0) + __log2f(n1)) - (__log2f(d0) + __log2f(d1));
+            n0 = d0 = 1.f;
+          }
+        }
+        {
+          const float sx = xn - zo.x, sy = yn - zo.y;
+          const float self = fmaf(sx, sx, fmaf(sy, sy, kTiny));
+          if (gl == im % G) part -= __log2f(self) + 64.f;  // log2(2^-64) = -64
         }
         part *= mf;
 

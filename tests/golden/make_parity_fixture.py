@@ -2,8 +2,8 @@
 Metropolis chain per basis row guided by |P_a Psi_m|^2, per-row ratio sums,
 reference normalisation and Hermitisation) run by the oracle's C restatement
 at the plain-method physics: m = 3, N = 8, V = omega r^2 + kappa r^4 with
-omega = 1e-2, kappa = 1e-4, sectors dL = 1..6, sigma = 0.3.  Eight
-independent replicas (seeds 1000..1007) give mean and standard deviation of
+omega = 1e-2, kappa = 1e-4, sectors dL = 1..6, sigma = 0.3.  Thirty-two
+independent replicas (seeds 1000..1031) give mean and standard deviation of
 every generalized eigenvalue and of the normalised matrices M and H.
 """
 import json
@@ -20,7 +20,7 @@ from oracle import oracle as O  # noqa: E402
 
 N, M_FILL, OMEGA, KAPPA, SIGMA = 8, 3, 1e-2, 1e-4, 0.3
 SECTORS = [1, 2, 3, 4, 5, 6]
-W, BURN, MEAS, REPS = 512, 500, 2000, 8
+W, BURN, MEAS, REPS = 512, 500, 2000, 32
 
 
 def main():
