@@ -74,8 +74,9 @@ struct GramJob {
 int launch_sweep(const SweepArgs& a, int lanes_per_walker, cudaStream_t st);
 size_t sweep_smem_bytes(int lanes_per_walker, int Npad);
 // Shared-memory layout of a walker: T2 slots per lane (ceil(N/G) rounded up
-// to even) and a per-walker stride Npad >= T2*G chosen so that the walker
-// groups of a half-warp hit disjoint bank pairs (Npad = G mod 16 for G < 16).
+// to even), stored as 16-byte slot-pair records, and an even per-walker stride
+// Npad >= T2*G (float2 units) chosen so that the walker groups of a
+// quarter-warp hit disjoint banks (Npad = 2G mod 16 for G < 8).
 void sweep_layout(int lanes_per_walker, int N, int* T2, int* Npad);
 bool sweep_config_ok(int lanes_per_walker, int N);
 

@@ -82,10 +82,27 @@ sweep_kernel(const SweepArgs a) {
   const bool live = w < a.W;
   const int N = a.N;
   const int T2 = a.T2;  // particle slots per lane, rounded up to even
-  float2* zs = sm_pos + (size_t)wl * a.Npad;
+  // Walker layout: lane gl owns particles j = gl + t G (slot t); slots 2q and
+  // 2q+1 of a lane form one 16-byte record {x_2q, x_2q+1, y_2q, y_2q+1} at
+  // float4 index q G + gl, so one load gives the x pair and the y pair.
+  float* zf = reinterpret_cast<float*>(sm_pos + (size_t)wl * a.Npad);
+  const float4* zs4 = reinterpret_cast<const float4*>(zf);
+  auto zoff = [](int j) {  // float offset of x_j (y_j at +2)
+    const int t = j / G;
+    return (((t >> 1) * G + (j % G)) << 2) + (t & 1);
+  };
+  auto ldz = [&](int j) {
+    const int o = zoff(j);
+    return make_float2(zf[o], zf[o + 2]);
+  };
+  auto stz = [&](int j, float2 z) {
+    const int o = zoff(j);
+    zf[o] = z.x;
+    zf[o + 2] = z.y;
+  };
 
   for (int j = gl; j < T2 * G; j += G)
-    zs[j] = (live && j < N) ? a.pos[(size_t)w * N + j] : make_float2(3.f * j + 1.f, 0.25f * j);
+    stz(j, (live && j < N) ? a.pos[(size_t)w * N + j] : make_float2(3.f * j + 1.f, 0.25f * j));
   __syncwarp();
 
   // ---- guide state: the distinct parts of the walker's guide partition ----
@@ -107,9 +124,14 @@ sweep_kernel(const SweepArgs a) {
     }
   }
 
-  const int tfull = N / G;                 // slots that hold a particle in every lane
-  const bool trem = tfull * G < N;         // a partly filled slot tfull follows
-  const bool rem_lane = gl < N - tfull * G;  // ... and holds a particle in this lane
+  // Slot pairs q < qfull hold particles in both slots in every lane; pair
+  // qfull (if any lane has a particle there) is masked per slot.
+  const int tfull = N / G;                   // slots that hold a particle in every lane
+  const int qfull = tfull >> 1;
+  const bool rem_lane = gl < N - tfull * G;  // slot tfull holds a particle in this lane
+  const bool tail0 = 2 * qfull < tfull || (2 * qfull == tfull && rem_lane);
+  const bool tail1 = 2 * qfull + 1 == tfull && rem_lane;
+  const bool tail = (tfull & 1) || tfull * G < N;  // lane 0 has a particle in pair qfull
   const float sigma = a.sigma;
   const float invR = a.invR;
   const float mf = float(a.m);
@@ -125,7 +147,7 @@ sweep_kernel(const SweepArgs a) {
         if (gk[t] > 0) {
           double2 acc = make_double2(0.0, 0.0);
           for (int j = 0; j < N; ++j) {
-            const float2 z = zs[j];
+            const float2 z = ldz(j);
             const double2 v = cpowi_d(make_float2(z.x * invR, z.y * invR), gk[t]);
             acc.x += v.x;
             acc.y += v.y;
@@ -147,7 +169,7 @@ sweep_kernel(const SweepArgs a) {
           const float rad = sqrtf(-2.f * logf(u1));
           float sn, cs;
           sincospif(2.f * u2, &sn, &cs);
-          const float2 zi = zs[i];
+          const float2 zi = ldz(i);
           pzx = zi.x + sigma * (rad * cs);
           pzy = zi.y + sigma * (rad * sn);
           plu = log2f(u3);
@@ -156,50 +178,48 @@ sweep_kernel(const SweepArgs a) {
       const int nb = min(G, N - i0);
       for (int b = 0; b < nb; ++b) {
         const int im = i0 + b;
-        const float2 zo = zs[im];
+        const float2 zo = ldz(im);
         const float xn = __shfl_sync(0xffffffffu, pzx, b, G);
         const float yn = __shfl_sync(0xffffffffu, pzy, b, G);
         const float lu = __shfl_sync(0xffffffffu, plu, b, G);
 
-        // Jastrow log2-ratio over this lane's particles j = gl + t G in two
-        // independent product chains, one log2 per chain every 16 slots
-        // (keeps FP32 in range).  No per-pair masks: every squared distance
-        // carries + 2^-64, which leaves any distance above 2^-40 unchanged and
-        // turns the self pair j == im into the factors (s + 2^-64) / 2^-64,
-        // removed once after the loop; the padding of the remainder slot is
-        // masked outside the loop.
+        // Jastrow log2-ratio over this lane's particles j = gl + t G: packed
+        // FP32x2 arithmetic on slot pairs, two product chains (even and odd
+        // slots), one log2 per chain every 16 slots (keeps FP32 in range).  No
+        // per-pair masks: every squared distance carries + 2^-64, which leaves
+        // any distance above 2^-40 unchanged and turns the self pair j == im
+        // into the factors (s + 2^-64) / 2^-64, removed once after the loop;
+        // the slots past the last full pair are masked outside the loop.
         float part = 0.f;
         {
-          float n0 = 1.f, d0 = 1.f;
-          if (trem) {  // slot tfull holds particles only in lanes gl < N - tfull G
-            const float2 za = zs[gl + tfull * G];
-            const float ax = xn - za.x, ay = yn - za.y, ex = zo.x - za.x, ey = zo.y - za.y;
-            const float pa = fmaf(ax, ax, fmaf(ay, ay, kTiny));
-            const float qa = fmaf(ex, ex, fmaf(ey, ey, kTiny));
-            n0 = rem_lane ? pa : 1.f;
-            d0 = rem_lane ? qa : 1.f;
+          const float2 XN = make_float2(xn, xn), YN = make_float2(yn, yn);
+          const float2 XO = make_float2(zo.x, zo.x), YO = make_float2(zo.y, zo.y);
+          const float2 M1 = make_float2(-1.f, -1.f), TN = make_float2(kTiny, kTiny);
+          auto factors = [&](int q, float2& pn, float2& po) {
+            const float4 P = zs4[q * G + gl];
+            const float2 X = make_float2(P.x, P.y), Y = make_float2(P.z, P.w);
+            const float2 ax = __ffma2_rn(X, M1, XN), ay = __ffma2_rn(Y, M1, YN);
+            const float2 ex = __ffma2_rn(X, M1, XO), ey = __ffma2_rn(Y, M1, YO);
+            pn = __ffma2_rn(ax, ax, __ffma2_rn(ay, ay, TN));
+            po = __ffma2_rn(ex, ex, __ffma2_rn(ey, ey, TN));
+          };
+          float2 n2 = make_float2(1.f, 1.f), d2 = n2;
+          if (tail) {  // slot pair qfull: a full slot and/or the partly filled slot
+            float2 pn, po;
+            factors(qfull, pn, po);
+            n2 = make_float2(tail0 ? pn.x : 1.f, tail1 ? pn.y : 1.f);
+            d2 = make_float2(tail0 ? po.x : 1.f, tail1 ? po.y : 1.f);
           }
-          for (int c0 = 0; c0 < tfull || c0 == 0; c0 += 16) {
-            float n1 = 1.f, d1 = 1.f;
-            const int cend = min(tfull, c0 + 16);
-            int t = c0;
-            for (; t + 1 < cend; t += 2) {
-              const float2 za = zs[gl + t * G], zb = zs[gl + (t + 1) * G];
-              const float ax = xn - za.x, ay = yn - za.y, ex = zo.x - za.x, ey = zo.y - za.y;
-              const float bx = xn - zb.x, by = yn - zb.y, fx = zo.x - zb.x, fy = zo.y - zb.y;
-              n0 *= fmaf(ax, ax, fmaf(ay, ay, kTiny));
-              d0 *= fmaf(ex, ex, fmaf(ey, ey, kTiny));
-              n1 *= fmaf(bx, bx, fmaf(by, by, kTiny));
-              d1 *= fmaf(fx, fx, fmaf(fy, fy, kTiny));
+          for (int q0 = 0; q0 < qfull || q0 == 0; q0 += 8) {
+            const int qend = min(qfull, q0 + 8);
+            for (int q = q0; q < qend; ++q) {
+              float2 pn, po;
+              factors(q, pn, po);
+              n2 = __fmul2_rn(n2, pn);
+              d2 = __fmul2_rn(d2, po);
             }
-            if (t < cend) {
-              const float2 za = zs[gl + t * G];
-              const float ax = xn - za.x, ay = yn - za.y, ex = zo.x - za.x, ey = zo.y - za.y;
-              n1 *= fmaf(ax, ax, fmaf(ay, ay, kTiny));
-              d1 *= fmaf(ex, ex, fmaf(ey, ey, kTiny));
-            }
-            part += (__log2f(n0) + __log2f(n1)) - (__log2f(d0) + __log2f(d1));
-            n0 = d0 = 1.f;
+            part += (__log2f(n2.x) + __log2f(n2.y)) - (__log2f(d2.x) + __log2f(d2.y));
+            n2 = d2 = make_float2(1.f, 1.f);
           }
         }
         {
@@ -233,7 +253,7 @@ sweep_kernel(const SweepArgs a) {
         const float gauss = (fmaf(zo.x, zo.x, zo.y * zo.y) - fmaf(xn, xn, yn * yn)) * (0.5f * kLog2e);
         const bool accept = (tot + gauss) >= lu;
         if (accept) {
-          if (gl == b) zs[im] = make_float2(xn, yn);
+          if (gl == b) stz(im, make_float2(xn, yn));
           ++nacc;
           if (row_guide) {
 #pragma unroll
@@ -246,7 +266,7 @@ sweep_kernel(const SweepArgs a) {
   }
 
   if (live) {
-    for (int j = gl; j < N; j += G) a.pos[(size_t)w * N + j] = zs[j];
+    for (int j = gl; j < N; j += G) a.pos[(size_t)w * N + j] = ldz(j);
     if (gl == 0 && a.accepted) a.accepted[w] += nacc;
   }
 
@@ -262,7 +282,7 @@ sweep_kernel(const SweepArgs a) {
   for (int q = 0; q < LEMC_MAX_PROBES; ++q) hc[q] = hs[q] = 0.f;
   const int K = a.K;
   for (int j = gl; j < N; j += G) {
-    const float2 z = zs[j];
+    const float2 z = ldz(j);
     const float2 wv = make_float2(z.x * invR, z.y * invR);
     float2 pw = wv;
 #pragma unroll
@@ -358,8 +378,10 @@ int launch_g(const SweepArgs& a, cudaStream_t st) {
 void sweep_layout(int G, int N, int* T2, int* Npad) {
   int t = (N + G - 1) / G;
   t += (t & 1);
-  int np = t * G;
-  if (G < 16) np += ((G - np) % 16 + 16) % 16;
+  int np = t * G;  // even: the 16-byte slot-pair records stay aligned
+  // For G < 8 a quarter-warp's 16-byte loads span 8 / G walkers of G * 16
+  // bytes each; a walker stride of 2G float2 mod 16 puts them in disjoint banks.
+  if (G < 8) np += ((2 * G - np) % 16 + 16) % 16;
   *T2 = t;
   *Npad = np;
 }
