@@ -709,9 +709,10 @@ int lemc_set_guide_rows(lemc_ctx* c, const int32_t* rows, int n_rows) {
   return upload_guide(c);
 }
 
-// Walker-width autotuner: times a few sweeps per feasible G on a copy of the
-// current walkers (restored afterwards, sweep counter unchanged) and keeps
-// the fastest.  Used when lanes_per_walker < 0.
+// Walker-width autotuner: times single sweeps per feasible G on a copy of the
+// current walkers (restored afterwards, sweep counter unchanged), measured
+// ones when the context has a basis, as a sampling step runs them, and keeps
+// the fastest (best of two rounds of three).  Used when lanes_per_walker < 0.
 static int autotune_lanes(lemc_ctx* c) {
   DevBuf<float2> save;
   LEMC_TRY(save.alloc(size_t(c->W) * c->N));
@@ -720,16 +721,21 @@ static int autotune_lanes(lemc_ctx* c) {
   const int keep_G = c->G;
   float best = 1e30f;
   int bestG = keep_G;
+  const int meas = (c->has_basis && c->rec_p.p && c->rec_w.p) ? 1 : 0;
   for (int G = 1; G <= 32; G *= 2) {
     if (!sweep_config_ok(G, c->N)) continue;
     c->G = G;
-    LEMC_TRY(sweep_once(c, 1, 0));  // warm the instruction cache / attributes
-    LEMC_CUDA(cudaEventRecord(c->ev[0], c->stream));
-    LEMC_TRY(sweep_once(c, 3, 0));
-    LEMC_CUDA(cudaEventRecord(c->ev[1], c->stream));
-    LEMC_CUDA(cudaEventSynchronize(c->ev[1]));
-    float ms = 0;
-    cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]);
+    LEMC_TRY(sweep_once(c, 1, meas));  // warm the instruction cache / attributes
+    float ms = 1e30f;
+    for (int rep = 0; rep < 2; ++rep) {
+      LEMC_CUDA(cudaEventRecord(c->ev[0], c->stream));
+      for (int k = 0; k < 3; ++k) LEMC_TRY(sweep_once(c, 1, meas));
+      LEMC_CUDA(cudaEventRecord(c->ev[1], c->stream));
+      LEMC_CUDA(cudaEventSynchronize(c->ev[1]));
+      float t = 0;
+      cudaEventElapsedTime(&t, c->ev[0], c->ev[1]);
+      ms = std::min(ms, t);
+    }
     if (ms < best) {
       best = ms;
       bestG = G;

@@ -66,7 +66,7 @@ __device__ __forceinline__ float group_sum(float v) {
   return v;
 }
 
-template <int G>
+template <int G, bool kRowGuide>
 __global__ void __launch_bounds__(kSweepThreads)
 sweep_kernel(const SweepArgs a) {
   constexpr int WPW = 32 / G;           // walkers per warp
@@ -106,7 +106,7 @@ sweep_kernel(const SweepArgs a) {
   __syncwarp();
 
   // ---- guide state: the distinct parts of the walker's guide partition ----
-  const bool row_guide = (a.guide == LEMC_GUIDE_ROW);
+  constexpr bool row_guide = kRowGuide;  // a.guide == LEMC_GUIDE_ROW
   int gk[GPL], gr[GPL];
   double2 gp[GPL];
 #pragma unroll
@@ -273,74 +273,68 @@ sweep_kernel(const SweepArgs a) {
   if (!a.measure) return;
 
   // ---- measurement record: p_k = sum_i (z_i / R)^k, k = 1..K, and weights ----
-  float2 acc[kMaxDegree];
-#pragma unroll
-  for (int k = 0; k < kMaxDegree; ++k) acc[k] = make_float2(0.f, 0.f);
-  float h2 = 0.f, h4 = 0.f;
-  float hc[LEMC_MAX_PROBES], hs[LEMC_MAX_PROBES];
-#pragma unroll
-  for (int q = 0; q < LEMC_MAX_PROBES; ++q) hc[q] = hs[q] = 0.f;
+  // Four degrees per pass over the particles (w^k by the same sequence of
+  // multiplications in every pass), then r^2 / r^4, then one pass per probe:
+  // few live registers, so the kernel's register count is set by the sweep.
   const int K = a.K;
-  for (int j = gl; j < N; j += G) {
-    const float2 z = ldz(j);
-    const float2 wv = make_float2(z.x * invR, z.y * invR);
-    float2 pw = wv;
+  for (int k0 = 0; k0 < K; k0 += 4) {
+    float2 acc[4];
 #pragma unroll
-    for (int k = 0; k < kMaxDegree; ++k) {
-      if (k < K) {
+    for (int k = 0; k < 4; ++k) acc[k] = make_float2(0.f, 0.f);
+    for (int j = gl; j < N; j += G) {
+      const float2 z = ldz(j);
+      const float2 wv = make_float2(z.x * invR, z.y * invR);
+      float2 pw = wv;
+      for (int k = 0; k < k0; ++k) pw = cmul(pw, wv);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
         acc[k].x += pw.x;
         acc[k].y += pw.y;
         pw = cmul(pw, wv);
       }
     }
-    const float r2 = fmaf(z.x, z.x, z.y * z.y);
-    h2 += r2;
-    h4 = fmaf(r2, r2, h4);
-    if (a.n_probes > 0) {
-      const float rinv = rsqrtf(r2);
-      const float2 u = make_float2(z.x * rinv, z.y * rinv);
 #pragma unroll
-      for (int q = 0; q < LEMC_MAX_PROBES; ++q) {
-        if (q < a.n_probes) {
-          const float2 e = cpowi(u, a.probes[q]);
-          hc[q] += e.x;
-          hs[q] += e.y;
-        }
-      }
+    for (int k = 0; k < 4; ++k) {
+      const float sx = group_sum<G>(acc[k].x), sy = group_sum<G>(acc[k].y);
+      if (live && k0 + k < K && ((k0 + k) % G) == gl)
+        a.rec_p[(size_t)(k0 + k) * a.W + w] = make_float2(sx, sy);
+    }
+  }
+  const size_t ldw = a.ldw;
+  {
+    float h2 = 0.f, h4 = 0.f;
+    for (int j = gl; j < N; j += G) {
+      const float2 z = ldz(j);
+      const float r2 = fmaf(z.x, z.x, z.y * z.y);
+      h2 += r2;
+      h4 = fmaf(r2, r2, h4);
+    }
+    h2 = group_sum<G>(h2);
+    h4 = group_sum<G>(h4);
+    if (live && gl == 0) {
+      a.rec_w[LEMC_W_ONE * ldw + w] = 1.f;
+      a.rec_w[LEMC_W_R2 * ldw + w] = h2;
+      a.rec_w[LEMC_W_R4 * ldw + w] = h4;
+      a.rec_w[LEMC_W_USER * ldw + w] = 0.f;
     }
   }
 #pragma unroll
-  for (int k = 0; k < kMaxDegree; ++k) {
-    if (k < K) {
-      acc[k].x = group_sum<G>(acc[k].x);
-      acc[k].y = group_sum<G>(acc[k].y);
+  for (int q = 0; q < LEMC_MAX_PROBES; ++q) {  // constant indices into the argument struct
+    if (q >= a.n_probes) break;
+    const int l = a.probes[q];
+    float hc = 0.f, hs = 0.f;
+    for (int j = gl; j < N; j += G) {
+      const float2 z = ldz(j);
+      const float rinv = rsqrtf(fmaf(z.x, z.x, z.y * z.y));
+      const float2 e = cpowi(make_float2(z.x * rinv, z.y * rinv), l);
+      hc += e.x;
+      hs += e.y;
     }
-  }
-  h2 = group_sum<G>(h2);
-  h4 = group_sum<G>(h4);
-#pragma unroll
-  for (int q = 0; q < LEMC_MAX_PROBES; ++q) {
-    if (q < a.n_probes) {
-      hc[q] = group_sum<G>(hc[q]);
-      hs[q] = group_sum<G>(hs[q]);
-    }
-  }
-  if (!live) return;
-#pragma unroll
-  for (int k = 0; k < kMaxDegree; ++k)
-    if (k < K && (k % G) == gl) a.rec_p[(size_t)k * a.W + w] = acc[k];
-  if (gl == 0) {
-    const size_t W = a.ldw;
-    a.rec_w[LEMC_W_ONE * W + w] = 1.f;
-    a.rec_w[LEMC_W_R2 * W + w] = h2;
-    a.rec_w[LEMC_W_R4 * W + w] = h4;
-    a.rec_w[LEMC_W_USER * W + w] = 0.f;
-#pragma unroll
-    for (int q = 0; q < LEMC_MAX_PROBES; ++q) {
-      if (q < a.n_probes) {
-        a.rec_w[(LEMC_W_PROBE0 + 2 * q) * W + w] = hc[q];
-        a.rec_w[(LEMC_W_PROBE0 + 2 * q + 1) * W + w] = hs[q];
-      }
+    hc = group_sum<G>(hc);
+    hs = group_sum<G>(hs);
+    if (live && gl == 0) {
+      a.rec_w[(LEMC_W_PROBE0 + 2 * q) * ldw + w] = hc;
+      a.rec_w[(LEMC_W_PROBE0 + 2 * q + 1) * ldw + w] = hs;
     }
   }
 }
@@ -358,19 +352,26 @@ __global__ void init_walkers_kernel(float2* pos, int W, int N, float radius, uin
   pos[t] = make_float2(rho * cs, rho * sn);
 }
 
-template <int G>
-int launch_g(const SweepArgs& a, cudaStream_t st) {
+template <int G, bool kRowGuide>
+int launch_gr(const SweepArgs& a, cudaStream_t st) {
   constexpr int WPB = (kSweepThreads / 32) * (32 / G);
   const size_t smem = size_t(WPB) * a.Npad * sizeof(float2);
   if (smem > 227 * 1024) return LEMC_ERR_CAPACITY;
   if (smem > 48 * 1024) {
-    if (cudaFuncSetAttribute(sweep_kernel<G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             int(smem)) != cudaSuccess)
+    if (cudaFuncSetAttribute(sweep_kernel<G, kRowGuide>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) != cudaSuccess)
       return LEMC_ERR_CUDA;
   }
   const int blocks = (a.W + WPB - 1) / WPB;
-  sweep_kernel<G><<<blocks, kSweepThreads, smem, st>>>(a);
+  sweep_kernel<G, kRowGuide><<<blocks, kSweepThreads, smem, st>>>(a);
   return cudaPeekAtLastError() == cudaSuccess ? LEMC_OK : LEMC_ERR_CUDA;
+}
+
+// the row-guide state (guide parts, power sums) only exists in the row-guide
+// instantiation, so the Laughlin-guide kernel runs with fewer registers
+template <int G>
+int launch_g(const SweepArgs& a, cudaStream_t st) {
+  return a.guide == LEMC_GUIDE_ROW ? launch_gr<G, true>(a, st) : launch_gr<G, false>(a, st);
 }
 
 }  // namespace
