@@ -14,11 +14,14 @@
 // whatever the weights are.  Weights are stored in BF16, arithmetic is FP32.
 //
 // Sampler layout: one walker per warp, positions in shared memory, lane l
-// owns particles l, l+32, ...  The 16 neighbours are found in 16 rounds of a
-// warp-wide minimum (redux.sync) over packed (distance^2, index) keys; each
-// lane evaluates two of the 64 hidden units of each layer; every reduction is
-// an xor butterfly, so all lanes hold bitwise identical values and take the
-// same accept decision.  Random numbers: Philox {i, sweep, walker, 4}.
+// owns particles l, l+32, ...  The 16 neighbours are found from packed
+// (distance^2, index) keys: each lane sorts its 8 keys once, then 16 rounds
+// of a warp-wide minimum (redux.sync) of the lane heads pop them in ascending
+// order.  Each lane evaluates two of the 64 hidden units of each layer with
+// packed FP32x2 arithmetic; the mean phi features reach all lanes through a
+// per-warp shared-memory buffer; every reduction is an xor butterfly, so all
+// lanes hold bitwise identical values and take the same accept decision.
+// Random numbers: Philox {i, sweep, walker, 4}.
 //
 // Training (evolution strategies + Adam, forward-only kernels): the objective
 // J = E[min(1, A) |z' - z_i|^2] over (configuration, particle, eps) samples
@@ -62,6 +65,34 @@ struct NetOut {
   float mr, mt, lr, lt;
 };
 
+// Shared-memory slot of canonical parameter k.  W2 ([kH][kIn]) is stored for
+// the packed rho layer: for input column v < 32 and lane l, the 16-byte record
+// (v * 32 + l) holds {W2[l][v], W2[l+32][v], W2[l][v+32], W2[l+32][v+32]};
+// column kH (the r/R weight) follows at kW2Packed + hidden unit.
+constexpr int kW2Packed = (kH / 2) * 32 * 4;
+static_assert(kH == 64, "the packed W2 layout assumes two hidden units per lane");
+__device__ __forceinline__ int p_slot(int k) {
+  if (k < kOffW2 || k >= kOffB2) return k;
+  const int e = k - kOffW2, h = e / kIn, c = e % kIn;
+  if (c == kH) return kOffW2 + kW2Packed + h;
+  return kOffW2 + ((((c & 31) * 32 + (h & 31)) << 2) | ((c >> 5) << 1) | (h >> 5));
+}
+
+// Ascending sort of a lane's 8 keys: Batcher's 19-comparator network.
+__device__ __forceinline__ void sort8(uint32_t* k) {
+  auto cx = [&](int i, int j) {
+    const uint32_t a = min(k[i], k[j]), b = max(k[i], k[j]);
+    k[i] = a;
+    k[j] = b;
+  };
+  cx(0, 2); cx(1, 3); cx(4, 6); cx(5, 7);
+  cx(0, 4); cx(1, 5); cx(2, 6); cx(3, 7);
+  cx(0, 1); cx(2, 3); cx(4, 5); cx(6, 7);
+  cx(2, 4); cx(3, 5);
+  cx(1, 4); cx(3, 6);
+  cx(1, 2); cx(3, 4); cx(5, 6);
+}
+
 __device__ __forceinline__ float warp_sum(float v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -70,8 +101,10 @@ __device__ __forceinline__ float warp_sum(float v) {
 
 // The network at centre zc for particle `self` of the walker whose positions
 // are zs[0..N).  All 32 lanes call it; every lane returns the same values.
+// P holds the parameters in their shared-memory slots (p_slot); gbuf is the
+// warp's 64-float shared scratch for the mean phi features.
 __device__ NetOut net_eval(const float* __restrict__ P, const float2* zs, int N, int self,
-                           float2 zc, float invR, int lane) {
+                           float2 zc, float invR, int lane, float* gbuf) {
   const float r2 = zc.x * zc.x + zc.y * zc.y;
   float c = 1.f, s = 0.f;
   if (r2 > 1e-20f) {
@@ -89,43 +122,59 @@ __device__ NetOut net_eval(const float* __restrict__ P, const float2* zs, int N,
       key[t] = (__float_as_uint(fmaf(dx, dx, dy * dy)) & 0xFFFFFF00u) | uint32_t(j);
     }
   }
-  const float w0x = P[kOffW1 + 2 * lane], w0y = P[kOffW1 + 2 * lane + 1], b0 = P[kOffB1 + lane];
-  const float w1x = P[kOffW1 + 2 * (lane + 32)], w1y = P[kOffW1 + 2 * (lane + 32) + 1];
-  const float b1 = P[kOffB1 + lane + 32];
-  float g0 = 0.f, g1 = 0.f;
+  // phi for this lane's hidden units lane and lane + 32, as one packed pair
+  const float2 W0X = make_float2(P[kOffW1 + 2 * lane], P[kOffW1 + 2 * (lane + 32)]);
+  const float2 W0Y = make_float2(P[kOffW1 + 2 * lane + 1], P[kOffW1 + 2 * (lane + 32) + 1]);
+  const float2 B0 = make_float2(P[kOffB1 + lane], P[kOffB1 + lane + 32]);
+  float2 g = make_float2(0.f, 0.f);
   int cnt = 0;
+  // The 16 nearest in ascending key order: each lane sorts its keys once, then
+  // every round takes the warp minimum of the lane heads and its lane pops it.
+  static_assert(kSlots == 8, "sort8 network");
+  sort8(key);
   for (int n = 0; n < kNbr; ++n) {
-    uint32_t lm = key[0];
-#pragma unroll
-    for (int t = 1; t < kSlots; ++t) lm = min(lm, key[t]);
-    const uint32_t m = __reduce_min_sync(0xffffffffu, lm);
+    const uint32_t m = __reduce_min_sync(0xffffffffu, key[0]);
     if (m == 0xFFFFFFFFu) break;
+    const bool pop = key[0] == m;  // keys are unique: exactly one lane pops
 #pragma unroll
-    for (int t = 0; t < kSlots; ++t)
-      if (key[t] == m) key[t] = 0xFFFFFFFFu;
+    for (int t = 0; t < kSlots - 1; ++t) key[t] = pop ? key[t + 1] : key[t];
+    key[kSlots - 1] = pop ? 0xFFFFFFFFu : key[kSlots - 1];
     const int j = int(m & 0xFFu);
     const float dx = zs[j].x - zc.x, dy = zs[j].y - zc.y;
     const float xr = (dx * c + dy * s) * kInScale, xt = (dy * c - dx * s) * kInScale;
-    g0 += fmaxf(fmaf(w0x, xr, fmaf(w0y, xt, b0)), 0.f);
-    g1 += fmaxf(fmaf(w1x, xr, fmaf(w1y, xt, b1)), 0.f);
+    const float2 h = __ffma2_rn(W0X, make_float2(xr, xr), __ffma2_rn(W0Y, make_float2(xt, xt), B0));
+    g = __fadd2_rn(g, make_float2(fmaxf(h.x, 0.f), fmaxf(h.y, 0.f)));
     ++cnt;
   }
   if (cnt > 0) {
     const float inv = 1.f / float(cnt);
-    g0 *= inv;
-    g1 *= inv;
+    g = __fmul2_rn(g, make_float2(inv, inv));
   }
   const float sf = sqrtf(r2) * invR - 1.f;
-  const float* w2a = P + kOffW2 + lane * kIn;
-  const float* w2b = P + kOffW2 + (lane + 32) * kIn;
-  float k0 = fmaf(w2a[kH], sf, P[kOffB2 + lane]);
-  float k1 = fmaf(w2b[kH], sf, P[kOffB2 + lane + 32]);
-#pragma unroll 8
-  for (int v = 0; v < 32; ++v) {
-    const float ga = __shfl_sync(0xffffffffu, g0, v), gb = __shfl_sync(0xffffffffu, g1, v);
-    k0 = fmaf(w2a[v], ga, fmaf(w2a[v + 32], gb, k0));
-    k1 = fmaf(w2b[v], ga, fmaf(w2b[v + 32], gb, k1));
+  // rho: the mean features reach every lane through shared memory (broadcast
+  // reads); each W2 record feeds two packed FMAs for units lane, lane + 32
+  __syncwarp();
+  gbuf[lane] = g.x;
+  gbuf[lane + 32] = g.y;
+  __syncwarp();
+  const float4* G4 = reinterpret_cast<const float4*>(gbuf);
+  const float4* W4 = reinterpret_cast<const float4*>(P + kOffW2) + lane;
+  float2 kk = make_float2(fmaf(P[kOffW2 + kW2Packed + lane], sf, P[kOffB2 + lane]),
+                          fmaf(P[kOffW2 + kW2Packed + lane + 32], sf, P[kOffB2 + lane + 32]));
+  auto rho_in = [&](int v, float ga, float gb) {
+    const float4 w = W4[v * 32];
+    kk = __ffma2_rn(make_float2(w.z, w.w), make_float2(gb, gb), kk);
+    kk = __ffma2_rn(make_float2(w.x, w.y), make_float2(ga, ga), kk);
+  };
+#pragma unroll 2
+  for (int v4 = 0; v4 < 8; ++v4) {
+    const float4 ga = G4[v4], gb = G4[8 + v4];
+    rho_in(4 * v4, ga.x, gb.x);
+    rho_in(4 * v4 + 1, ga.y, gb.y);
+    rho_in(4 * v4 + 2, ga.z, gb.z);
+    rho_in(4 * v4 + 3, ga.w, gb.w);
   }
+  float k0 = kk.x, k1 = kk.y;
   k0 = fmaxf(k0, 0.f);
   k1 = fmaxf(k1, 0.f);
   float o[4];
@@ -145,9 +194,9 @@ struct Move {
 };
 
 __device__ Move propose(const float* __restrict__ P, const float2* zs, int N, int i, float invR,
-                        float m, float e_r, float e_t, int lane) {
+                        float m, float e_r, float e_t, int lane, float* gbuf) {
   const float2 zo = zs[i];
-  const NetOut f = net_eval(P, zs, N, i, zo, invR, lane);
+  const NetOut f = net_eval(P, zs, N, i, zo, invR, lane, gbuf);
   const float sr = __expf(f.lr), st = __expf(f.lt);
   const float dr = fmaf(sr, e_r, f.mr), dt = fmaf(st, e_t, f.mt);
   const float r2 = zo.x * zo.x + zo.y * zo.y;
@@ -161,7 +210,7 @@ __device__ Move propose(const float* __restrict__ P, const float2* zs, int N, in
   mv.zn = make_float2(zo.x + (c * dr - s * dt), zo.y + (s * dr + c * dt));
   const float log_qf = -0.5f * (e_r * e_r + e_t * e_t) - f.lr - f.lt;
   // reverse proposal: the network at the proposed configuration
-  const NetOut b = net_eval(P, zs, N, i, mv.zn, invR, lane);
+  const NetOut b = net_eval(P, zs, N, i, mv.zn, invR, lane, gbuf);
   const float rn2 = mv.zn.x * mv.zn.x + mv.zn.y * mv.zn.y;
   float cb = 1.f, sb = 0.f;
   if (rn2 > 1e-20f) {
@@ -199,12 +248,13 @@ __device__ __forceinline__ void box_muller(uint32_t a, uint32_t b, float& e0, fl
 }
 
 __device__ void load_params(float* P, const __nv_bfloat16* w) {
-  for (int k = threadIdx.x; k < kNParams; k += blockDim.x) P[k] = __bfloat162float(w[k]);
+  for (int k = threadIdx.x; k < kNParams; k += blockDim.x) P[p_slot(k)] = __bfloat162float(w[k]);
 }
 
 __global__ void __launch_bounds__(kWarpsPerBlock * 32)
 learned_sweep_kernel(const SweepArgs a, const __nv_bfloat16* __restrict__ wts) {
-  __shared__ float P[kNParams];
+  __shared__ __align__(16) float P[kNParams];
+  __shared__ __align__(16) float gsm[kWarpsPerBlock][kH];
   extern __shared__ float2 zsm[];
   load_params(P, wts);
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -226,7 +276,7 @@ learned_sweep_kernel(const SweepArgs a, const __nv_bfloat16* __restrict__ wts) {
       const U4 r = philox4x32_10(U4{uint32_t(i), sweep, uint32_t(w), kTagLearned}, a.seed_lo, a.seed_hi);
       float er, et;
       box_muller(r.x, r.y, er, et);
-      const Move mv = propose(P, zs, N, i, a.invR, m, er, et, lane);
+      const Move mv = propose(P, zs, N, i, a.invR, m, er, et, lane, gsm[wib]);
       const bool acc = __logf(u01(r.z)) < mv.log_a;
       __syncwarp();
       if (acc) {
@@ -239,72 +289,69 @@ learned_sweep_kernel(const SweepArgs a, const __nv_bfloat16* __restrict__ wts) {
   for (int j = lane; j < N; j += 32) a.pos[size_t(w) * N + j] = zs[j];
   if (a.accepted && lane == 0) a.accepted[w] += nacc;
   if (!a.measure) return;
-  // measurement record, the plain sweep's layout
-  float2 acc[kMaxDegree];
+  // measurement record, the plain sweep's layout: four degrees per pass over
+  // the particles (w^k by the same sequence of multiplications in every pass),
+  // then r^2 / r^4, then one pass per probe, so that few registers are live
+  const int K = a.K;
+  for (int k0 = 0; k0 < K; k0 += 4) {
+    float2 acc[4];
 #pragma unroll
-  for (int k = 0; k < kMaxDegree; ++k) acc[k] = make_float2(0.f, 0.f);
-  float h2 = 0.f, h4 = 0.f, hc[LEMC_MAX_PROBES], hs[LEMC_MAX_PROBES];
+    for (int k = 0; k < 4; ++k) acc[k] = make_float2(0.f, 0.f);
+    for (int j = lane; j < N; j += 32) {
+      const float2 z = zs[j];
+      const float2 wv = make_float2(z.x * a.invR, z.y * a.invR);
+      float2 pw = wv;
+      for (int k = 0; k < k0; ++k)
+        pw = make_float2(pw.x * wv.x - pw.y * wv.y, pw.x * wv.y + pw.y * wv.x);
 #pragma unroll
-  for (int q = 0; q < LEMC_MAX_PROBES; ++q) hc[q] = hs[q] = 0.f;
-  for (int j = lane; j < N; j += 32) {
-    const float2 z = zs[j];
-    const float2 wv = make_float2(z.x * a.invR, z.y * a.invR);
-    float2 pw = wv;
-#pragma unroll
-    for (int k = 0; k < kMaxDegree; ++k) {
-      if (k < a.K) {
+      for (int k = 0; k < 4; ++k) {
         acc[k].x += pw.x;
         acc[k].y += pw.y;
         pw = make_float2(pw.x * wv.x - pw.y * wv.y, pw.x * wv.y + pw.y * wv.x);
       }
     }
-    const float r2 = fmaf(z.x, z.x, z.y * z.y);
-    h2 += r2;
-    h4 = fmaf(r2, r2, h4);
-    if (a.n_probes > 0) {
-      const float th = atan2f(z.y, z.x);
 #pragma unroll
-      for (int q = 0; q < LEMC_MAX_PROBES; ++q) {
-        if (q < a.n_probes) {
-          float sn, cs;
-          sincosf(float(a.probes[q]) * th, &sn, &cs);
-          hc[q] += cs;
-          hs[q] += sn;
-        }
-      }
+    for (int k = 0; k < 4; ++k) {
+      const float sx = warp_sum(acc[k].x), sy = warp_sum(acc[k].y);
+      if (k0 + k < K && ((k0 + k) & 31) == lane)
+        a.rec_p[size_t(k0 + k) * a.W + w] = make_float2(sx, sy);
+    }
+  }
+  const size_t ldw = a.ldw;
+  {
+    float h2 = 0.f, h4 = 0.f;
+    for (int j = lane; j < N; j += 32) {
+      const float2 z = zs[j];
+      const float r2 = fmaf(z.x, z.x, z.y * z.y);
+      h2 += r2;
+      h4 = fmaf(r2, r2, h4);
+    }
+    h2 = warp_sum(h2);
+    h4 = warp_sum(h4);
+    if (lane == 0) {
+      a.rec_w[LEMC_W_ONE * ldw + w] = 1.f;
+      a.rec_w[LEMC_W_R2 * ldw + w] = h2;
+      a.rec_w[LEMC_W_R4 * ldw + w] = h4;
+      a.rec_w[LEMC_W_USER * ldw + w] = 0.f;
     }
   }
 #pragma unroll
-  for (int k = 0; k < kMaxDegree; ++k) {
-    if (k < a.K) {
-      acc[k].x = warp_sum(acc[k].x);
-      acc[k].y = warp_sum(acc[k].y);
+  for (int q = 0; q < LEMC_MAX_PROBES; ++q) {  // constant indices into the argument struct
+    if (q >= a.n_probes) break;
+    const float l = float(a.probes[q]);
+    float hc = 0.f, hs = 0.f;
+    for (int j = lane; j < N; j += 32) {
+      const float2 z = zs[j];
+      float sn, cs;
+      sincosf(l * atan2f(z.y, z.x), &sn, &cs);
+      hc += cs;
+      hs += sn;
     }
-  }
-  h2 = warp_sum(h2);
-  h4 = warp_sum(h4);
-#pragma unroll
-  for (int q = 0; q < LEMC_MAX_PROBES; ++q) {
-    if (q < a.n_probes) {
-      hc[q] = warp_sum(hc[q]);
-      hs[q] = warp_sum(hs[q]);
-    }
-  }
-#pragma unroll
-  for (int k = 0; k < kMaxDegree; ++k)
-    if (k < a.K && (k & 31) == lane) a.rec_p[size_t(k) * a.W + w] = acc[k];
-  if (lane == 0) {
-    const size_t W = a.ldw;
-    a.rec_w[LEMC_W_ONE * W + w] = 1.f;
-    a.rec_w[LEMC_W_R2 * W + w] = h2;
-    a.rec_w[LEMC_W_R4 * W + w] = h4;
-    a.rec_w[LEMC_W_USER * W + w] = 0.f;
-#pragma unroll
-    for (int q = 0; q < LEMC_MAX_PROBES; ++q) {
-      if (q < a.n_probes) {
-        a.rec_w[(LEMC_W_PROBE0 + 2 * q) * W + w] = hc[q];
-        a.rec_w[(LEMC_W_PROBE0 + 2 * q + 1) * W + w] = hs[q];
-      }
+    hc = warp_sum(hc);
+    hs = warp_sum(hs);
+    if (lane == 0) {
+      a.rec_w[(LEMC_W_PROBE0 + 2 * q) * ldw + w] = hc;
+      a.rec_w[(LEMC_W_PROBE0 + 2 * q + 1) * ldw + w] = hs;
     }
   }
 }
@@ -315,7 +362,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
 learned_eval_kernel(const float2* __restrict__ cfgs, int n, int N, float invR, float m,
                     const int32_t* __restrict__ particle, const float* __restrict__ eps,
                     const __nv_bfloat16* __restrict__ wts, float* __restrict__ out) {
-  __shared__ float P[kNParams];
+  __shared__ __align__(16) float P[kNParams];
+  __shared__ __align__(16) float gsm[kWarpsPerBlock][kH];
   extern __shared__ float2 zsm[];
   load_params(P, wts);
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -327,8 +375,8 @@ learned_eval_kernel(const float2* __restrict__ cfgs, int n, int N, float invR, f
   if (sidx >= n) return;
   __syncwarp();
   const int i = particle[sidx];
-  const NetOut f = net_eval(P, zs, N, i, zs[i], invR, lane);
-  const Move mv = propose(P, zs, N, i, invR, m, eps[2 * sidx], eps[2 * sidx + 1], lane);
+  const NetOut f = net_eval(P, zs, N, i, zs[i], invR, lane, gsm[wib]);
+  const Move mv = propose(P, zs, N, i, invR, m, eps[2 * sidx], eps[2 * sidx + 1], lane, gsm[wib]);
   if (lane == 0) {
     float* o = out + size_t(sidx) * 8;
     o[0] = f.mr;
@@ -348,7 +396,8 @@ __global__ void __launch_bounds__(kTrainWarps * 32)
 es_objective_kernel(const float2* __restrict__ cfgs, int n_cfg, int N, float invR, float m,
                     const float* __restrict__ theta, float es_sigma, uint32_t step, uint32_t k0,
                     uint32_t k1, int batch, double* __restrict__ J) {
-  __shared__ float P[kNParams];
+  __shared__ __align__(16) float P[kNParams];
+  __shared__ __align__(16) float gsm[kTrainWarps][kH];
   __shared__ float part[kTrainWarps];
   extern __shared__ float2 zsm[];
   const int pert = blockIdx.y;
@@ -358,7 +407,7 @@ es_objective_kernel(const float2* __restrict__ cfgs, int n_cfg, int N, float inv
     const U4 r = philox4x32_10(U4{uint32_t(k), uint32_t(pair), step, kTagEs}, k0, k1);
     float e0, e1;
     box_muller(r.x, r.y, e0, e1);
-    P[k] = theta[k] + sgn * e0;
+    P[p_slot(k)] = theta[k] + sgn * e0;
   }
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int sidx = blockIdx.x * kTrainWarps + wib;
@@ -373,7 +422,7 @@ es_objective_kernel(const float2* __restrict__ cfgs, int n_cfg, int N, float inv
   if (live) {
     float er, et;
     box_muller(r.z, r.w, er, et);
-    const Move mv = propose(P, zs, N, i, invR, m, er, et, lane);
+    const Move mv = propose(P, zs, N, i, invR, m, er, et, lane, gsm[wib]);
     val = (mv.log_a >= 0.f ? 1.f : __expf(mv.log_a)) * mv.jump2;
     if (!(val == val)) val = 0.f;
   }
@@ -584,7 +633,14 @@ extern "C" int lemc_proposal_train(lemc_proposal* p, const void* configs, int n_
   if (tc->steps < 1 || tc->batch < 1 || tc->pairs < 1 || !(tc->lr > 0.f) || !(tc->es_sigma > 0.f))
     return LEMC_ERR_ARG;
   const int N = p->N;
-  if (walker_smem(N, kTrainWarps) > 48 * 1024 - sizeof(float) * kNParams) return LEMC_ERR_CAPACITY;
+  // static shared memory of es_objective_kernel: parameters, phi scratch, partial sums
+  const size_t smem_static = sizeof(float) * (kNParams + kTrainWarps * kH + kTrainWarps);
+  const size_t smem_dyn = walker_smem(N, kTrainWarps);
+  if (smem_static + smem_dyn > 227 * 1024) return LEMC_ERR_CAPACITY;
+  if (smem_static + smem_dyn > 48 * 1024 &&
+      cudaFuncSetAttribute(es_objective_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           int(smem_dyn)) != cudaSuccess)
+    return LEMC_ERR_CUDA;
   if (p->J_cap < 2 * tc->pairs) {
     cudaFree(p->J);
     p->J = nullptr;
