@@ -72,7 +72,7 @@ sweep_kernel(const SweepArgs a) {
   constexpr int WPW = 32 / G;           // walkers per warp
   constexpr int WPB = (kSweepThreads / 32) * WPW;
   constexpr int GPL = (kMaxGuideParts + G - 1) / G;  // guide slots per lane
-  extern __shared__ float2 sm_pos[];
+  extern __shared__ __align__(16) float2 sm_pos[];  // 16-byte slot-pair records
 
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
