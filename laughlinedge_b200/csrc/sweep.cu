@@ -273,28 +273,30 @@ sweep_kernel(const SweepArgs a) {
   if (!a.measure) return;
 
   // ---- measurement record: p_k = sum_i (z_i / R)^k, k = 1..K, and weights ----
-  // Four degrees per pass over the particles (w^k by the same sequence of
-  // multiplications in every pass), then r^2 / r^4, then one pass per probe:
-  // few live registers, so the kernel's register count is set by the sweep.
+  // kPassDeg degrees per pass over the particles (w^k by the same sequence of
+  // multiplications in every pass; two passes for K = 12), then r^2 / r^4,
+  // then one pass per probe: few live registers, so the kernel's register
+  // count is set by the sweep.
+  constexpr int kPassDeg = 6;
   const int K = a.K;
-  for (int k0 = 0; k0 < K; k0 += 4) {
-    float2 acc[4];
+  for (int k0 = 0; k0 < K; k0 += kPassDeg) {
+    float2 acc[kPassDeg];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) acc[k] = make_float2(0.f, 0.f);
+    for (int k = 0; k < kPassDeg; ++k) acc[k] = make_float2(0.f, 0.f);
     for (int j = gl; j < N; j += G) {
       const float2 z = ldz(j);
       const float2 wv = make_float2(z.x * invR, z.y * invR);
       float2 pw = wv;
       for (int k = 0; k < k0; ++k) pw = cmul(pw, wv);
 #pragma unroll
-      for (int k = 0; k < 4; ++k) {
+      for (int k = 0; k < kPassDeg; ++k) {
         acc[k].x += pw.x;
         acc[k].y += pw.y;
         pw = cmul(pw, wv);
       }
     }
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
+    for (int k = 0; k < kPassDeg; ++k) {
       const float sx = group_sum<G>(acc[k].x), sy = group_sum<G>(acc[k].y);
       if (live && k0 + k < K && ((k0 + k) % G) == gl)
         a.rec_p[(size_t)(k0 + k) * a.W + w] = make_float2(sx, sy);
