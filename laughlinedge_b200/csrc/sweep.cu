@@ -8,13 +8,16 @@
 //
 // Layout: a walker is a group of G consecutive lanes (G in {1,..,32}; G = 32
 // is one walker per warp).  The walker's coordinates live in shared memory;
-// lane l of the group owns particles j = l, l+G, l+2G, ...  For a move of
+// lane l of the group owns particles j = l, l+G, l+2G, ... (slots 0, 1, 2,
+// ...), stored as 16-byte records of two slots {x, x', y, y'}.  For a move of
 // particle i every lane accumulates the products prod |z'-z_j|^2 and
-// prod |z-z_j|^2 over its particles in two independent chains (one log2 per
-// chain every 16 slots keeps FP32 in range), the G partial log-ratios are
-// combined with a butterfly of
+// prod |z-z_j|^2 over its particles with packed FP32x2 arithmetic, even and
+// odd slots in the two halves (one log2 per chain every 16 slots keeps FP32
+// in range); the G partial log-ratios are combined with a butterfly of
 // __shfl_xor_sync (all lanes end with bitwise identical sums, hence identical
-// accept decisions), and the owner lane commits the move.
+// accept decisions), and the owner lane commits the move.  The row-guide
+// state exists only in the row-guide instantiation (kRowGuide), so the
+// Laughlin-guide kernel keeps its register count, and occupancy, low.
 //
 // Random numbers: one Philox-4x32-10 call per proposed move,
 // counter = {i, sweep, walker, 0}: (u1, u2) -> Box-Muller step, u3 -> the
