@@ -1,23 +1,34 @@
 #!/usr/bin/env python
-"""Benchmark of the LaughlinEdge B200 engine on the mixed-precision workload.
+"""Benchmark of the LaughlinEdge B200 engine.
 
-Workload (one GPU): Laughlin nu = 1/3 (m = 3), N = 50 electrons, confinement
-V = omega r^2 + kappa r^4 with omega = 5e-3, kappa = 2e-5, edge sectors
-dL = 0..12 (272 power-sum states), 65536 walkers, Gaussian step sigma = 0.3,
-Philox seed 42, basis in FP32 with (z/R)^k scaling, S/H contraction in
-TF32 hi/lo split precision on tcgen05 with FP32 accumulation flushed to FP64.
-Synthetic by construction: walkers start uniformly in the disk of radius
-sqrt(2 m N) and are burnt in before timing.
+Default line: the learned-proposal form (the workload the metric "effective
+samples/s and S/H updates/s, learned vs plain MC" is quoted on).  Laughlin
+nu = 1/3 (m = 3), N = 200 electrons, V = omega r^2 + kappa r^4 with
+omega = 1e-3, kappa = 5e-6, edge sectors dL = 1..20 (2713 power-sum states),
+65536 walkers, Philox seed 42.  The DeepSets proposal is trained first (5000
+ES+Adam steps on 2^20 configurations of the plain chain).  Synthetic by
+construction: walkers start uniformly in the disk of radius sqrt(2 m N) and are
+burnt in before anything is timed.
 
 A step is one pass of the hot path over all walkers: one Metropolis sweep
 (N single-particle moves per walker), one measurement record, the basis build
-and the S, H2, H4 contraction.  Metric: effective samples/s
-= walkers x steps / tau_int / time, tau_int the integrated autocorrelation time
-(in sweeps) of p_1..p_4, max over the four, measured on the timed steps.
+and the TF32x3 contraction of S, H2, H4 for every sector.  The same step is
+timed with three samplers: the learned proposal, the plain Gaussian step at
+the same sigma = 0.3, and the plain step tuned to 50 % acceptance (the
+reference's own criterion).
+
+Metric: effective samples/s = walkers x steps / tau_int / time.  tau_int (in
+sweeps, max over Re/Im p_1..p_4) comes from a separate, untimed chain of the
+same sampler, thousands of sweeps long (>= 50 tau), by Sokal's windowing with
+a binning plateau beside it; it is never estimated from the timed steps.
 
 ``--impl reference`` times the oracle's C restatement of the reference
 estimator (one Metropolis chain per basis row guided by |P_a Psi|^2, per-row
-ratio sums) on all host cores, on a bounded sample of the same workload.
+ratio sums) on all host cores on a bounded sample of the same workload, with
+tau_int from a long chain of that estimator.
+``--mixed`` gives the mixed-precision line (N = 50, dL = 0..12, 272 states),
+``--batched`` the batched line (N = 100, dL = 1..20, 16 kappas) and
+``--evolution`` the time-evolution pipeline, each as its own JSON line.
 """
 from __future__ import annotations
 
@@ -35,16 +46,18 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 WORKLOAD = {
+    "workload": "learned_proposal_m3_N200_dL1-20_W65536",
+    "particles": 200, "inverse_filling": 3, "omega": 1e-3, "kappa": 5e-6,
+    "sectors": list(range(1, 21)), "walkers": 65536, "sigma": 0.3, "seed": 42,
+    "gram_mode": "tf32x3", "train_configs": 1 << 20, "train_steps": 5000, "train_batch": 1024,
+    "train_pairs": 32, "tau_walkers": 8192, "tau_sweeps_plain": 6000, "tau_sweeps_learned": 3000,
+    "burn": 1000,
+}
+MIXED = {
     "workload": "mixed_precision_m3_N50_dL0-12_W65536",
-    "particles": 50,
-    "inverse_filling": 3,
-    "omega": 5e-3,
-    "kappa": 2e-5,
-    "sectors": list(range(13)),
-    "walkers": 65536,
-    "sigma": 0.3,
-    "seed": 42,
-    "gram_mode": "tf32x3",
+    "particles": 50, "inverse_filling": 3, "omega": 5e-3, "kappa": 2e-5,
+    "sectors": list(range(13)), "walkers": 65536, "sigma": 0.3, "seed": 42,
+    "gram_mode": "tf32x3", "tau_walkers": 8192, "tau_sweeps": 4000, "burn": 1000,
 }
 METRIC = "effective_samples_per_s"
 UNIT = "samples/s"
@@ -158,46 +171,175 @@ def traffic_from_profiles():
     return out
 
 
-def cpu_baseline(w, steps_hint=None, threads=0, budget_s=15.0):
-    """The oracle's restatement of the reference estimator on the host cores."""
+def cpu_port(w, threads=0, budget_s=15.0, tau_sweeps=2000, tau_sectors=(1, 2, 3, 4)):
+    """The oracle's C restatement of the reference estimator (one Metropolis
+    chain per basis row guided by |P_a Psi|^2, per-row ratio sums over every
+    row of the workload's sectors) on the host cores.
+
+    Throughput: a bounded sample (about budget_s of CPU work) of the full
+    workload.  tau_int: a separate chain of the same estimator and step,
+    tau_sweeps measured sweeps long with one walker per thread (the guide rows
+    of tau_sectors; the p_1..p_4 series does not depend on the basis size),
+    Sokal windowing with the binning plateau beside it."""
+    import numpy as np
+
+    import laughlinedge_b200 as L
     from oracle import oracle as O
     O.load()
     nth = threads or O.load().orc_max_threads()
     N, m = w["particles"], w["inverse_filling"]
+    t0 = time.perf_counter()
+    tres = O.run_rows(N, m, nth, w["sigma"], w["seed"] + 5, 200, tau_sweeps, list(tau_sectors),
+                      nthreads=nth)
+    t_tau = time.perf_counter() - t0
+    tau = L.sampler.series_tau(np.asarray(tres["series"]))
     # calibrate on a tiny run, then size the sample to the budget
-    wc = 8 * nth
+    wc = nth
     t0 = time.perf_counter()
-    O.run_rows(N, m, wc, w["sigma"], w["seed"], 10, 30, w["sectors"], nthreads=nth)
-    per = (time.perf_counter() - t0) / (wc * 40)  # seconds per walker-sweep (all cores)
-    n_meas = int(steps_hint or 1000)
-    W = max(nth, int(budget_s / max(per, 1e-9) / (n_meas + 50)))
-    W = min(W, 4096)
+    O.run_rows(N, m, wc, w["sigma"], w["seed"], 2, 3, w["sectors"], nthreads=nth)
+    per = (time.perf_counter() - t0) / (wc * 5)  # seconds per walker-sweep (all cores)
+    n_meas = 20
+    W = max(nth, min(4096, int(budget_s / max(per, 1e-9) / (n_meas + 5))))
+    W -= W % nth
     t0 = time.perf_counter()
-    res = O.run_rows(N, m, W, w["sigma"], w["seed"], 50, n_meas, w["sectors"], nthreads=nth)
+    O.run_rows(N, m, W, w["sigma"], w["seed"], 5, n_meas, w["sectors"], nthreads=nth)
     dt = time.perf_counter() - t0
-    taus = O.tau_int(res["series"])
-    tau = float(max(0.5 * (taus[2 * k] + taus[2 * k + 1]) for k in range(4)))
-    value = W * n_meas / tau / dt
-    return {"value": value, "unit": UNIT, "cores": nth, "kind": "port",
-            "sample": f"{W} walkers x ({n_meas} measured + 50 burn-in) sweeps of the per-row "
-                      f"reference estimator, all 272 rows, tau_int={tau:.2f} sweeps, "
-                      f"{dt:.1f} s wall", "walker_sweeps_per_s": W * (n_meas + 50) / dt,
-            "tau_int": tau}
+    D = sum_d2(w["sectors"], N)[1]
+    ws_per_s = W * (n_meas + 5) / dt
+    return {"value": ws_per_s / tau["sokal"], "unit": UNIT, "cores": nth, "kind": "port",
+            "sample": f"{W} walkers x ({n_meas} measured + 5 burn-in) sweeps of the per-row reference "
+                      f"estimator over all {D} rows, {dt:.1f} s wall; tau_int from a separate "
+                      f"{tau_sweeps}-sweep chain of {nth} walkers ({t_tau:.1f} s)",
+            "walker_sweeps_per_s": ws_per_s, "tau_int": tau["sokal"], "tau_int_detail": tau}
 
 
 def run_reference(args, ws, rank):
     if rank != 0:
         return
-    w = WORKLOAD
-    cb = cpu_baseline(w, steps_hint=min(max(args.steps, 200), 2000))
+    w = MIXED if args.mixed else WORKLOAD
+    cb = cpu_port(w)
     line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT,
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": {k: w[k] for k in ("workload", "particles", "inverse_filling", "walkers")},
+            "data": "synthetic",
+            "config": {k: w[k] for k in ("workload", "particles", "inverse_filling", "walkers")},
             "cpu_baseline": cb,
             "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def long_chain_tau(L, cfg, sectors, n_burn, n_meas, proposal=None, init_xy=None, tune=None):
+    """tau_int of a sampler from a separate untimed chain: n_burn unmeasured and
+    n_meas measured sweeps; the walker-mean p_1..p_4 series gives Sokal and
+    binning estimates.  tune = (target, tol) tunes the step first."""
+    smp = L.Sampler(cfg, sectors)
+    if proposal is not None:
+        smp.set_proposal(proposal)
+    smp.init_walkers(init_xy)
+    tuned = None
+    if tune is not None:
+        tuned = smp.tune_step(*tune)
+    smp.run(n_burn, measure=False)
+    smp.reset()
+    smp.run(n_meas, measure=True)
+    out = L.sampler.series_tau(smp.series())
+    out["acceptance"] = smp.stats().acceptance
+    if tuned is not None:
+        out["sigma"] = tuned[0]
+    smp.close()
+    return out
+
+
+def timed_steps(L, torch, cfg, sectors, steps, warmup, proposal=None, init_xy=None, clocks_index=None):
+    """K full steps (sweep + record + basis + contraction of every sector) on the
+    context stream, CUDA events around them; returns (ms, stats, clocks)."""
+    smp = L.Sampler(cfg, sectors)
+    if proposal is not None:
+        smp.set_proposal(proposal)
+    smp.init_walkers(init_xy)
+    smp.run(warmup, measure=True)
+    smp.reset()
+    st_ = torch.cuda.ExternalStream(smp.stream())
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    smp.synchronize()
+    torch.cuda.synchronize()
+    clk = Clocks(clocks_index) if clocks_index is not None else None
+    a.record(st_)
+    smp.run(steps, measure=True)
+    b.record(st_)
+    b.synchronize()
+    clocks = clk.stop() if clk else None
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b)
+    stats = smp.stats()
+    smp.close()
+    return ms, stats, clocks
+
+
+def kernel_profile(L, cfg, sectors, steps, proposal=None, init_xy=None, burn=0):
+    """Per-kernel device times (ms per launch) from a profiled pass: CUDA events
+    between the sweep, basis and contraction launches of each step."""
+    pc = dict(cfg.__dict__)
+    pc.update(profile=True, graph_batch=0)
+    smp = L.Sampler(L.SamplerConfig(**pc), sectors)
+    if proposal is not None:
+        smp.set_proposal(proposal)
+    smp.init_walkers(init_xy)
+    if burn:
+        smp.run(burn, measure=False)
+    smp.run(steps, measure=True)
+    st = smp.stats()
+    smp.close()
+    return st.ms_sweep / steps, st.ms_basis / steps, st.ms_gram / steps
+
+
+def learned_move_flop(N, k_nn=16, hidden=64):
+    """Algorithmic FP32 FLOP of one learned move: two network evaluations
+    (forward at z, reverse at z') of phi (k_nn x 2 -> hidden), rho (hidden+1 ->
+    hidden) and the head (hidden -> 4), 2 FLOP per multiply-add; the two kNN
+    distance scans (3 FLOP per other particle each) and the Jastrow ratio (12
+    FLOP per pair term)."""
+    net = 2 * (k_nn * 2 * hidden + (hidden + 1) * hidden + hidden * 4)
+    return 2 * net + 2 * 3 * (N - 1) + 12 * (N - 1)
+
+
+def rooflines(L, w, mode, t_sweep, t_basis, t_gram, learned, clocks):
+    peaks, peak_kind = measured_peaks()
+    N, W = w["particles"], w["walkers"]
+    sd2, D = sum_d2(w["sectors"], N)
+    K = max(4, max(w["sectors"]))
+    fp32_peak = 148 * 128 * 2 * peaks.get("sm_max_mhz", 1965.0) / 1e6  # TFLOP/s, nominal at max clock
+    if learned:
+        flop_sweep = W * N * learned_move_flop(N)
+    else:
+        flop_sweep = W * (12.0 * N * (N - 1) + N * (16.0 * K + 40.0))
+    bytes_basis = W * (8.0 * D + 8.0 * K)
+    flop_gram = W * 8.0 * 3 * sd2
+    traffic = traffic_from_profiles()
+    tag = w["workload"]
+    tf32_peak = peaks["bf16_tflops"] / 2.0 if mode == L._lib.GRAM_TF32X3 else peaks["bf16_tflops"]
+    roofs = {
+        "sweep": {"bound": "fp32", "achieved": flop_sweep / (t_sweep * 1e-3) / 1e12,
+                  "peak": fp32_peak, "unit": "TFLOP/s",
+                  "peak_source": "nominal FP32 (148 SMs x 128 lanes x 2 x max SM clock)",
+                  "kernel": "learned_sweep_kernel" if learned else "sweep_kernel",
+                  "traffic": traffic.get(("learned_sweep" if learned else "sweep") + "@" + tag),
+                  "ms_per_launch": t_sweep},
+        "basis": {"bound": "hbm", "achieved": bytes_basis / (t_basis * 1e-3) / 1e9,
+                  "peak": peaks["hbm_gbs"], "unit": "GB/s", "peak_source": f"{peak_kind} hbm_gbs",
+                  "kernel": "basis_kernel", "traffic": traffic.get("basis@" + tag),
+                  "ms_per_launch": t_basis},
+        "gram": {"bound": "tensor", "achieved": flop_gram / (t_gram * 1e-3) / 1e12,
+                 "peak": tf32_peak, "unit": "TFLOP/s",
+                 "peak_source": (f"{peak_kind} bf16_tflops / 2 (dense TF32 rate)" if mode == L._lib.GRAM_TF32X3
+                                 else f"{peak_kind} bf16_tflops"),
+                 "kernel": "gram_tc_kernel", "traffic": traffic.get("gram@" + tag),
+                 "ms_per_launch": t_gram},
+    }
+    for r in roofs.values():
+        r["frac"] = r["achieved"] / r["peak"]
+    return roofs
 
 
 def run_ours(args, ws, rank, local):
@@ -210,240 +352,201 @@ def run_ours(args, ws, rank, local):
     N, m, W = w["particles"], w["inverse_filling"], w["walkers"]
     mode = gram_mode_id(args.gram or w["gram_mode"])
     seed = w["seed"] + 1000003 * rank
-    cfg = L.SamplerConfig(N, m, W, step_sigma=w["sigma"], seed=seed, lanes_per_walker=-1,
-                          gram_mode=mode, graph_batch=args.graph_batch)
-    smp = L.Sampler(cfg, w["sectors"])
-    smp.init_walkers()
-    smp.run(args.burn, measure=False)
-    smp.run(args.warmup, measure=True)
-    smp.reset()
-    stream = torch.cuda.ExternalStream(smp.stream())
-    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sectors = w["sectors"]
+    gb = args.graph_batch
+
+    # 1) burnt-in plain chain: the common start of every sampler, and the
+    #    training configurations of the proposal
+    plain0 = L.Sampler(L.SamplerConfig(N, m, W, step_sigma=w["sigma"], seed=seed,
+                                       lanes_per_walker=-1), [1, 2, 3, 4])
+    plain0.init_walkers()
+    plain0.run(args.burn, measure=False)
+    G = plain0.lanes_per_walker()
+    n_snap = w["train_configs"] // W
+    cfg_buf = torch.empty((n_snap * W, N, 2), dtype=torch.float32, device="cuda")
+    for k in range(n_snap):
+        plain0.run(10, measure=False)
+        plain0.copy_positions_device(cfg_buf[k * W:(k + 1) * W].data_ptr())
+    start_xy = plain0.positions()
+    plain0.close()
+    prop = L.LearnedProposal(N, m, init_sigma=w["sigma"], seed=w["seed"])
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    trace = prop.train(cfg_buf.data_ptr(), cfg_buf.shape[0], steps=w["train_steps"],
+                       batch=w["train_batch"], pairs=w["train_pairs"], lr=3e-3, es_sigma=0.02,
+                       seed=w["seed"])
+    t_train = time.perf_counter() - t0
+    del cfg_buf
+
+    # 2) tau_int of each sampler from separate untimed long chains
+    Wt = w["tau_walkers"]
+    tau_xy = start_xy[:Wt]
+    mk = lambda WW, sg, lanes=G, **kw: L.SamplerConfig(N, m, WW, step_sigma=sg, seed=seed + 7,
+                                                        lanes_per_walker=lanes, **kw)
+    tau_plain = long_chain_tau(L, mk(Wt, w["sigma"]), [1, 2, 3, 4], 200, w["tau_sweeps_plain"],
+                               init_xy=tau_xy)
+    tau_tuned = long_chain_tau(L, mk(Wt, w["sigma"]), [1, 2, 3, 4], 200, w["tau_sweeps_plain"],
+                               init_xy=tau_xy, tune=(0.5, 0.01))
+    sigma_tuned = tau_tuned["sigma"]
+    tau_learned = long_chain_tau(L, mk(Wt, w["sigma"], lanes=0), [1, 2, 3, 4], 200,
+                                 w["tau_sweeps_learned"], proposal=prop, init_xy=tau_xy)
+
+    # 3) timed full steps of each sampler at W = 65536, all 20 sectors
+    full = lambda sg: L.SamplerConfig(N, m, W, step_sigma=sg, seed=seed + 11, lanes_per_walker=G,
+                                      gram_mode=mode, graph_batch=gb)
     if ws > 1:
         torch.distributed.barrier()
-    torch.cuda.synchronize()
-    clk = Clocks(local)
-    start.record(stream)
-    smp.run(args.steps, measure=True)
-    end.record(stream)
-    end.synchronize()
-    clocks = clk.stop()
-    torch.cuda.synchronize()
-    ms = start.elapsed_time(end)
+    ms_l, st_l, clocks = timed_steps(L, torch, full(w["sigma"]), sectors, args.steps, args.warmup,
+                                     proposal=prop, init_xy=start_xy, clocks_index=local)
+    ms_p, st_p, _ = timed_steps(L, torch, full(w["sigma"]), sectors, args.steps, args.warmup,
+                                init_xy=start_xy)
+    ms_t, st_t, _ = timed_steps(L, torch, full(sigma_tuned), sectors, args.steps, args.warmup,
+                                init_xy=start_xy)
     if ws > 1:
         torch.distributed.barrier()
-    st = smp.stats()
-    tau = st.tau_int
-    ms_max = allreduce_max(ms, ws)
-    sd2, D = sum_d2(w["sectors"], N)
-    total_samples = W * args.steps * ws
-    value = total_samples / tau / (ms_max * 1e-3)
-    sh_updates = total_samples * sd2 * 3 / (ms_max * 1e-3)
+    ms_max = allreduce_max(ms_l, ws)
+    sd2, D = sum_d2(sectors, N)
+    total = W * args.steps * ws
+    value = total / tau_learned["sokal"] / (ms_max * 1e-3)
+    arms = {}
+    for name, ms, tau, st, sg in (("learned", ms_max, tau_learned, st_l, w["sigma"]),
+                                  ("plain_equal_sigma", allreduce_max(ms_p, ws), tau_plain, st_p, w["sigma"]),
+                                  ("plain_tuned_sigma", allreduce_max(ms_t, ws), tau_tuned, st_t, sigma_tuned)):
+        arms[name] = {"effective_samples_per_s": total / tau["sokal"] / (ms * 1e-3),
+                      "ms_per_step": ms / args.steps, "sigma": sg, "tau_int": tau["sokal"],
+                      "tau_int_chain": tau, "acceptance_timed": st.acceptance,
+                      "walker_sweeps_per_s": total / (ms * 1e-3)}
+    sh_updates = total * sd2 * 3 / (ms_max * 1e-3)
 
-    # per-kernel device times (separate profiled pass, events between kernels)
-    G = smp.lanes_per_walker()
-    psmp = L.Sampler(L.SamplerConfig(N, m, W, step_sigma=w["sigma"], seed=seed + 7,
-                                     lanes_per_walker=G, gram_mode=mode,
-                                     profile=True), w["sectors"])
-    psmp.init_walkers()
-    psmp.run(args.burn // 4, measure=False)
-    npro = min(200, max(20, args.steps // 5))
-    psmp.run(npro, measure=True)
-    pst = psmp.stats()
-    t_sweep, t_basis, t_gram = pst.ms_sweep / npro, pst.ms_basis / npro, pst.ms_gram / npro
-    psmp.close()
-
-    peaks, peak_kind = measured_peaks()
-    K = max(4, max(w["sectors"]))
-    clk_ghz = (clocks or {}).get("sm_mhz", peaks.get("sm_max_mhz", 1965.0)) / 1e3
-    fp32_peak = 148 * 128 * 2 * peaks.get("sm_max_mhz", 1965.0) / 1e6  # TFLOP/s, nominal at max clock
-    flop_sweep = W * (12.0 * N * (N - 1) + N * (16.0 * K + 40.0))
-    bytes_basis = W * (8.0 * D + 8.0 * K)
-    flop_gram = W * 8.0 * 3 * sd2
-    traffic = traffic_from_profiles()
-    tf32_peak = peaks["bf16_tflops"] / 2.0 if mode == L._lib.GRAM_TF32X3 else peaks["bf16_tflops"]
-    roofs = {
-        "sweep": {"bound": "fp32", "achieved": flop_sweep / (t_sweep * 1e-3) / 1e12,
-                  "peak": fp32_peak, "unit": "TFLOP/s",
-                  "peak_source": "nominal FP32 (148 SMs x 128 lanes x 2 x max SM clock)",
-                  "traffic": traffic.get("sweep"), "ms_per_launch": t_sweep},
-        "basis": {"bound": "hbm", "achieved": bytes_basis / (t_basis * 1e-3) / 1e9,
-                  "peak": peaks["hbm_gbs"], "unit": "GB/s", "peak_source": f"{peak_kind} hbm_gbs",
-                  "traffic": traffic.get("basis"), "ms_per_launch": t_basis},
-        "gram": {"bound": "tensor", "achieved": flop_gram / (t_gram * 1e-3) / 1e12,
-                 "peak": tf32_peak, "unit": "TFLOP/s",
-                 "peak_source": (f"{peak_kind} bf16_tflops / 2 (dense TF32 rate)" if mode == L._lib.GRAM_TF32X3
-                                 else f"{peak_kind} bf16_tflops"),
-                 "traffic": traffic.get("gram"), "ms_per_launch": t_gram},
-    }
-    for r in roofs.values():
-        r["frac"] = r["achieved"] / r["peak"]
+    # 4) per-kernel device times (profiled pass) and rooflines, learned and plain
+    npro = 5
+    ks_l = kernel_profile(L, full(w["sigma"]), sectors, npro, proposal=prop, init_xy=start_xy)
+    ks_p = kernel_profile(L, full(w["sigma"]), sectors, npro, init_xy=start_xy)
+    roofs = rooflines(L, w, mode, *ks_l, True, clocks)
+    roofs_plain = rooflines(L, w, mode, *ks_p, False, clocks)
     dominant = max(roofs, key=lambda k: roofs[k]["ms_per_launch"])
-    G = smp.lanes_per_walker()
-    smp.close()
+    # the mixed-precision workload's rooflines (N = 50, dL = 0..12), plain sampler
+    wm = MIXED
+    cm = L.SamplerConfig(wm["particles"], m, wm["walkers"], step_sigma=wm["sigma"], seed=seed,
+                         lanes_per_walker=4, gram_mode=mode)
+    ks_m = kernel_profile(L, cm, wm["sectors"], 20, burn=400)
+    roofs_mixed = rooflines(L, wm, mode, *ks_m, False, None)
 
-    # end-to-end through the public API with host buffers
-    e2e = None
-    if rank == 0 or ws > 1:
-        g = np.random.default_rng(seed)
-        r0 = math.sqrt(2 * m * N)
-        rr = r0 * np.sqrt(g.random((W, N)))
-        th = 2 * math.pi * g.random((W, N))
-        host = torch.from_numpy(np.stack([rr * np.cos(th), rr * np.sin(th)], -1).astype(np.float32)).pin_memory()
-        e_steps = max(50, args.steps // 4)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        esmp = L.Sampler(L.SamplerConfig(N, m, W, step_sigma=w["sigma"], seed=seed + 11,
-                                         lanes_per_walker=G, gram_mode=mode),
-                         w["sectors"])
-        esmp.init_walkers(host.numpy())
-        for _ in range(e_steps):
-            esmp.run(1, measure=True)  # per step: device work + d2h of the step's series entry
-        grams = [esmp.gram(s) for s in range(len(w["sectors"]))]
-        for s, (S, H2, H4, _) in enumerate(grams):
-            Mn, Hn = L.normalise(S, H2, H4, w["omega"], w["kappa"])
-        t_e2e = time.perf_counter() - t0
-        etau = esmp.stats().tau_int
-        esmp.close()
-        h2d = W * N * 8
-        d2h = 64 * e_steps + sum(3 * 16 * g_[0].size for g_ in grams)
-        # tau_int is a property of the chain, not of the call path: the same
-        # estimate (from the longer device-timed run) converts both arms, the
-        # shorter run's own estimate is reported beside it.
-        e2e = {"value": W * e_steps * ws / tau / t_e2e, "unit": UNIT,
-               "h2d_bytes_per_step": h2d / e_steps, "d2h_bytes_per_step": d2h / e_steps,
-               "steps": e_steps, "tau_int_used": tau, "tau_int_this_run": etau,
-               "note": "lemc_create + init from pinned host positions + per-step lemc_run(1) with "
-                       "series read-back + Gram read-back + normalisation, wall clock"}
-
+    # 5) end to end through the public API with host buffers (learned sampler)
+    e_steps = max(10, min(args.steps, 40))
+    host = torch.from_numpy(start_xy).pin_memory()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    esmp = L.Sampler(L.SamplerConfig(N, m, W, step_sigma=w["sigma"], seed=seed + 13,
+                                     lanes_per_walker=G, gram_mode=mode), sectors)
+    esmp.set_proposal(prop)
+    esmp.init_walkers(host.numpy())
+    for _ in range(e_steps):
+        esmp.run(1, measure=True)  # per step: device work + d2h of the step's series entry
+    grams = [esmp.gram(s) for s in range(len(sectors))]
+    for S, H2, H4, _ in grams:
+        L.normalise(S, H2, H4, w["omega"], w["kappa"])
+    t_e2e = time.perf_counter() - t0
+    esmp.close()
+    h2d = W * N * 8
+    d2h = 64 * e_steps + sum(3 * 16 * g_[0].size for g_ in grams)
+    e2e = {"value": W * e_steps * ws / tau_learned["sokal"] / t_e2e, "unit": UNIT,
+           "h2d_bytes_per_step": h2d / e_steps, "d2h_bytes_per_step": d2h / e_steps,
+           "steps": e_steps, "tau_int_used": tau_learned["sokal"],
+           "note": "lemc_create + init from pinned host positions + per-step lemc_run(1) with "
+                   "series read-back + Gram read-back and normalisation of 20 sectors, wall clock"}
+    prop.close()
     if rank != 0:
         return
     cb = None
     if not args.no_cpu_baseline:
         try:
-            cb = cpu_baseline(w, steps_hint=min(args.steps, 1000))
+            cb = cpu_port(w)
+            cb["tau_int_gpu_plain_same_sigma"] = tau_plain["sokal"]
         except Exception as exc:  # the baseline is reported, never required
             cb = {"error": str(exc)}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32+tf32x3" if mode == L._lib.GRAM_TF32X3 else "f32",
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+bf16-net+tf32x3" if mode == L._lib.GRAM_TF32X3 else "f32+bf16-net",
         "data": "synthetic",
         "config": {"workload": w["workload"], "particles": N, "inverse_filling": m,
-                   "sectors": "0..12", "basis_states": D, "walkers_per_gpu": W,
-                   "sigma": w["sigma"], "gram_mode": args.gram or w["gram_mode"],
-                   "lanes_per_walker": G, "graph_batch": args.graph_batch,
-                   "l2": "inputs larger than L2 (V planes 143 MB per step)",
+                   "omega": w["omega"], "kappa": w["kappa"], "sectors": "1..20",
+                   "basis_states": D, "sum_d2": sd2, "walkers_per_gpu": W, "sigma": w["sigma"],
+                   "sampler": "learned DeepSets proposal (exact MH)",
+                   "gram_mode": args.gram or w["gram_mode"], "lanes_per_walker_plain": G,
+                   "graph_batch": gb, "l2": "inputs larger than L2 (V planes 1.4 GB per step)",
                    "parallelism": f"replicas x{ws} (walkers sharded, no collective)"},
-        "tau_int": tau, "tau_int_each": list(st.tau_int_each), "acceptance": st.acceptance,
-        "sh_updates_per_s": sh_updates, "walker_sweeps_per_s": total_samples / (ms_max * 1e-3),
-        "kernel_ms": {"sweep": t_sweep, "basis": t_basis, "gram": t_gram},
-        "roofline": dict(roofs[dominant], kernel=dominant),
-        "rooflines": roofs,
+        "tau_int": tau_learned["sokal"],
+        "tau_source": f"Sokal window on a separate untimed chain: {Wt} walkers, "
+                      f"{w['tau_sweeps_learned']} measured sweeps after 200 burn-in, from the "
+                      f"burnt-in plain configurations (binning plateau beside it)",
+        "samplers": arms,
+        "learned_over_plain_equal_sigma": arms["learned"]["effective_samples_per_s"] /
+        arms["plain_equal_sigma"]["effective_samples_per_s"],
+        "learned_over_plain_tuned_sigma": arms["learned"]["effective_samples_per_s"] /
+        arms["plain_tuned_sigma"]["effective_samples_per_s"],
+        "sh_updates_per_s": sh_updates, "walker_sweeps_per_s": total / (ms_max * 1e-3),
+        "kernel_ms": {"sweep": ks_l[0], "basis": ks_l[1], "gram": ks_l[2]},
+        "roofline": dict(roofs[dominant], which=dominant),
+        "rooflines": roofs, "rooflines_plain_sampler": roofs_plain,
+        "rooflines_mixed_precision_N50": dict(roofs_mixed, workload=wm["workload"]),
+        "train_seconds": t_train,
+        "train_objective_first_last": [float(np.mean(trace[:50])), float(np.mean(trace[-50:]))],
         "clocks": clocks,
-        "gpu_launches": 3 * args.steps,
+        # per step: sweep, basis, contraction (+ the counter kernel inside a graph)
+        "gpu_launches": (4 * (args.steps // gb) * gb + 3 * (args.steps % gb)) if gb else 3 * args.steps,
         "e2e": e2e,
         "cpu_baseline": cb,
     }
     print(json.dumps(line), flush=True)
 
 
-LEARNED = {
-    "workload": "learned_proposal_m3_N200",
-    "particles": 200, "inverse_filling": 3, "omega": 1e-3, "kappa": 5e-6,
-    "sigma": 0.3, "walkers": 65536, "tau_walkers": 8192, "seed": 42,
-    "train_configs": 1 << 20, "train_steps": 5000, "train_batch": 1024, "train_pairs": 32,
-}
-
-
-def run_learned(args, rank, local):
-    """Learned vs plain single-particle proposal at equal sigma (N=200, m=3).
-
-    One line: walker-sweeps/s of each sampler (sweep kernel only, W=65536,
-    CUDA events), tau_int of p_1..p_4 of each (W=8192 chains, 1500 measured
-    sweeps after burn-in), effective samples/s = walker-sweeps/s / tau_int,
-    acceptance, and the training cost (5000 ES+Adam steps on 2^20
-    configurations drawn from the plain sampler)."""
-    if rank != 0:
-        return
+def run_mixed(args, ws, rank, local):
+    """Mixed-precision line: N = 50, dL = 0..12 (272 states), plain step
+    sigma = 0.3, TF32x3 contraction, W = 65536; tau_int from a separate
+    4000-sweep chain."""
     import numpy as np
     import torch
 
     import laughlinedge_b200 as L
-    w = LEARNED
+    w = MIXED
     torch.cuda.set_device(local)
     N, m, W = w["particles"], w["inverse_filling"], w["walkers"]
-    sectors = [1, 2, 3, 4]
-
-    def timed_sweeps(smp, n):
-        st = torch.cuda.ExternalStream(smp.stream())
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        smp.synchronize()
-        a.record(st)
-        smp.run(n, measure=False)
-        b.record(st)
-        b.synchronize()
-        return a.elapsed_time(b) / 1e3
-
-    # training data: snapshots of the plain chain
-    plain = L.Sampler(L.SamplerConfig(N, m, W, step_sigma=w["sigma"], seed=w["seed"],
-                                      lanes_per_walker=-1), sectors)
-    plain.init_walkers()
-    plain.run(args.burn + 100, measure=False)
-    n_snap = w["train_configs"] // W
-    cfg = torch.empty((n_snap * W, N, 2), dtype=torch.float32, device="cuda")
-    for k in range(n_snap):
-        plain.run(10, measure=False)
-        plain.copy_positions_device(cfg[k * W:(k + 1) * W].data_ptr())
-    plain.synchronize()
-    t_plain = timed_sweeps(plain, 20) / 20
-    plain.close()
-
-    prop = L.LearnedProposal(N, m, init_sigma=w["sigma"], seed=w["seed"])
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    trace = prop.train(cfg.data_ptr(), cfg.shape[0], steps=w["train_steps"], batch=w["train_batch"],
-                       pairs=w["train_pairs"], lr=3e-3, es_sigma=0.02, seed=w["seed"])
-    t_train = time.perf_counter() - t0
-    del cfg
-
-    lsmp = L.Sampler(L.SamplerConfig(N, m, W, step_sigma=w["sigma"], seed=w["seed"] + 1), sectors)
-    lsmp.set_proposal(prop)
-    lsmp.init_walkers()
-    lsmp.run(50, measure=False)
-    t_learned = timed_sweeps(lsmp, 5) / 5
-    lsmp.close()
-
-    def tau_run(use_prop):
-        smp = L.Sampler(L.SamplerConfig(N, m, w["tau_walkers"], step_sigma=w["sigma"],
-                                        seed=w["seed"] + 7, lanes_per_walker=0), sectors)
-        if use_prop:
-            smp.set_proposal(prop)
-        smp.init_walkers()
-        smp.run(args.burn + 400, measure=False)
-        smp.run(1500, measure=True)
-        st = smp.stats()
-        out = {"tau_int": st.tau_int, "tau_int_each": list(st.tau_int_each),
-               "acceptance": st.acceptance}
-        smp.close()
-        return out
-
-    tp, tl = tau_run(False), tau_run(True)
-    res = {}
-    for name, t, tau in (("plain", t_plain, tp), ("learned", t_learned, tl)):
-        ws_s = W / t
-        res[name] = dict(tau, walker_sweeps_per_s=ws_s, ms_per_sweep=1e3 * t,
-                         effective_samples_per_s=ws_s / tau["tau_int"])
-    line = {"metric": "effective_samples_per_s", "workload": w["workload"], "n_gpus": 1,
-            "unit": "samples/s", "higher_is_better": True, "data": "synthetic",
-            "config": {k: w[k] for k in w if k != "workload"},
-            "plain": res["plain"], "learned": res["learned"],
-            "learned_over_plain": res["learned"]["effective_samples_per_s"] /
-            res["plain"]["effective_samples_per_s"],
-            "tau_ratio_plain_over_learned": tp["tau_int"] / tl["tau_int"],
-            "train_seconds": t_train,
-            "train_objective_first_last": [float(np.mean(trace[:50])), float(np.mean(trace[-50:]))]}
-    prop.close()
+    mode = gram_mode_id(args.gram or w["gram_mode"])
+    seed = w["seed"] + 1000003 * rank
+    p0 = L.Sampler(L.SamplerConfig(N, m, W, step_sigma=w["sigma"], seed=seed, lanes_per_walker=-1),
+                   [1, 2, 3, 4])
+    p0.init_walkers()
+    p0.run(args.burn, measure=False)
+    G = p0.lanes_per_walker()
+    start_xy = p0.positions()
+    p0.close()
+    tau = long_chain_tau(L, L.SamplerConfig(N, m, w["tau_walkers"], step_sigma=w["sigma"],
+                                            seed=seed + 7, lanes_per_walker=G),
+                         [1, 2, 3, 4], 200, w["tau_sweeps"], init_xy=start_xy[:w["tau_walkers"]])
+    cfg = L.SamplerConfig(N, m, W, step_sigma=w["sigma"], seed=seed + 11, lanes_per_walker=G,
+                          gram_mode=mode, graph_batch=args.graph_batch)
+    ms, st, clocks = timed_steps(L, torch, cfg, w["sectors"], args.steps, args.warmup,
+                                 init_xy=start_xy, clocks_index=local)
+    ms_max = allreduce_max(ms, ws)
+    sd2, D = sum_d2(w["sectors"], N)
+    total = W * args.steps * ws
+    ks = kernel_profile(L, cfg, w["sectors"], 40, init_xy=start_xy)
+    roofs = rooflines(L, w, mode, *ks, False, clocks)
+    dominant = max(roofs, key=lambda k: roofs[k]["ms_per_launch"])
+    if rank != 0:
+        return
+    line = {"metric": METRIC, "value": total / tau["sokal"] / (ms_max * 1e-3), "unit": UNIT,
+            "workload": w["workload"], "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_max / args.steps, "higher_is_better": True, "data": "synthetic",
+            "dtype": "f32+tf32x3", "config": {k: w[k] for k in w if k != "sectors"},
+            "tau_int": tau["sokal"], "tau_int_chain": tau, "acceptance": st.acceptance,
+            "sh_updates_per_s": total * sd2 * 3 / (ms_max * 1e-3),
+            "walker_sweeps_per_s": total / (ms_max * 1e-3),
+            "kernel_ms": {"sweep": ks[0], "basis": ks[1], "gram": ks[2]},
+            "roofline": dict(roofs[dominant], which=dominant), "rooflines": roofs, "clocks": clocks}
     print(json.dumps(line), flush=True)
 
 
@@ -518,29 +621,33 @@ def run_batched(args, rank, local):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=2000)
-    ap.add_argument("--warmup", type=int, default=20)
-    ap.add_argument("--burn", type=int, default=400, help="untimed burn-in sweeps")
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--burn", type=int, default=1000, help="untimed burn-in sweeps")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--gram", default=None, choices=["fp64", "bf16x3", "bf16x4", "tf32x3"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mixed", action="store_true",
+                    help="mixed-precision form N=50, dL 0..12 (its own JSON line)")
     ap.add_argument("--batched", action="store_true",
                     help="batched form N=100, dL 1..20, 16 kappas (its own JSON line)")
-    ap.add_argument("--learned", action="store_true",
-                    help="learned vs plain proposal at N=200 (its own JSON line)")
-    ap.add_argument("--graph-batch", type=int, default=32,
-                    help="measured sweeps per CUDA-graph replay in the timed run (0: direct launches)")
+    ap.add_argument("--evolution", action="store_true",
+                    help="time-evolution pipeline N=100, dL 0,2..16 (its own JSON line)")
+    ap.add_argument("--graph-batch", type=int, default=4,
+                    help="measured steps per CUDA-graph replay in the timed run (0: direct launches)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     ws, rank, local = dist_init()
     try:
-        if args.learned:
-            run_learned(args, rank, local)
+        if args.impl == "reference":
+            run_reference(args, ws, rank)
         elif args.batched:
             run_batched(args, rank, local)
-        elif args.impl == "reference":
-            run_reference(args, ws, rank)
+        elif args.evolution:
+            run_evolution(args, rank, local)
+        elif args.mixed:
+            run_mixed(args, ws, rank, local)
         else:
             run_ours(args, ws, rank, local)
     finally:

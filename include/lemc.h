@@ -137,6 +137,16 @@ LEMC_API int lemc_create(const lemc_config* cfg, lemc_ctx** out);
 LEMC_API int lemc_destroy(lemc_ctx* ctx);
 /* Gaussian step sigma of subsequent sweeps (step tuning). */
 LEMC_API int lemc_set_step(lemc_ctx* ctx, float sigma);
+/* Tune the Gaussian step to an acceptance within tol of target: measure the
+ * acceptance of `moves` unmeasured sweeps of the live chain at the current
+ * step, double or halve the step until the target is bracketed, then regula
+ * falsi on the bracket (at most 40 + 60 measurements).  The walkers advance and
+ * the accumulators are reset.  On success the context keeps the step, and
+ * *sigma / *acceptance (may be NULL) receive it and its last measured
+ * acceptance; LEMC_ERR_NUMERIC when the search fails.  Replaces optimal_step
+ * and mcmc_acceptanceBisection (modules/edge_mc/em_bisection.cu:7-153). */
+LEMC_API int lemc_tune_step(lemc_ctx* ctx, double target, double tol, int moves, float* sigma,
+                            double* acceptance);
 /* Walker width G in use (after autotuning). */
 LEMC_API int lemc_lanes_per_walker(const lemc_ctx* ctx, int* lanes);
 /* Select the angular-momentum sectors whose basis is sampled. */
@@ -212,6 +222,22 @@ LEMC_API int lemc_read_stats(lemc_ctx* ctx, lemc_stats* st);
 LEMC_API int lemc_read_positions(lemc_ctx* ctx, float* host_xy);
 /* Walker-mean series of Re/Im p_1..p_4 per measurement: series[m*8 + 2(k-1) + c]. */
 LEMC_API int lemc_read_series(lemc_ctx* ctx, double* series, int max_meas, int* n_meas);
+
+/* ---- error analysis of a scalar Monte Carlo series (host only) -------------
+ * The reference leaves error bars to post-processing of repeated runs
+ * (main.cu:18-20, em_spectrum.cu:393-414); these give them from one run.
+ * Sokal's windowed integrated autocorrelation time: tau = 1/2 + sum_{t<=M}
+ * rho(t) with the smallest window M >= c tau (c <= 0 selects 5).  *tau is NaN
+ * when no window up to T/2 qualifies, T < 100 or T < 50 max(tau, 1): the series is too short
+ * for its own autocorrelation time, and no estimate is claimed.  lemc_stats
+ * reports this estimate (max over Re/Im p_1..p_4), NaN under the same rule. */
+LEMC_API int lemc_tau_sokal(const double* x, int T, double c, double* tau);
+/* Binning analysis: bins of length 2^k while at least min_bins bins remain
+ * (<= 0 selects 16); tau(b) = b s_b^2 / (2 s_1^2) at the last level, its error,
+ * the standard error of the series mean from that level, and *converged = 1
+ * when the last two levels agree within twice the error (or 5 %). */
+LEMC_API int lemc_tau_binning(const double* x, int T, int min_bins, double* tau,
+                              double* tau_err, double* err_of_mean, int* converged);
 
 /* ---- device-buffer entry points (the hot path, for integrators/tests) ------
  * All pointers are device pointers; `stream` is a cudaStream_t (NULL = legacy).
@@ -328,6 +354,11 @@ LEMC_API int lemc_occupation(const lemc_occupation_config* cfg, double* out, dou
  * Set-up: the first call on each device resolves the array's device address
  * with that device current (cudaGetSymbolAddress), which can load the module
  * onto the device.  Make that first call before any stream capture.
+ *
+ * Footprint: the array is part of the library's device module, so its
+ * LEMC_OCC_STATIC_SCRATCH_BYTES are reserved on every device where the module
+ * is loaded (by any entry point of the library, not only this one), until the
+ * process exits.
  *
  * Concurrency: every call on one device uses the same array, so calls that
  * overlap on the same device (from several host threads) race and corrupt

@@ -98,11 +98,14 @@ _SIGNATURES = {
     "lemc_read_cross": ([_P, _I, _I, _DP, _DP, _DP], _I),
     "lemc_read_rows": ([_P, _D, _D, _DP, _DP, _DP, _DP, _DP, _DP, _DP], _I),
     "lemc_set_step": ([_P, C.c_float], _I),
+    "lemc_tune_step": ([_P, _D, _D, _I, _FP, _DP], _I),
     "lemc_occupation": ([C.POINTER(OccConfig), _DP, _DP], _I),
     "lemc_occupation_static": ([C.POINTER(OccConfig), _DP, _DP], _I),
     "lemc_read_stats": ([_P, C.POINTER(Stats)], _I),
     "lemc_read_positions": ([_P, _FP], _I),
     "lemc_read_series": ([_P, _DP, _I, _IP], _I),
+    "lemc_tau_sokal": ([_DP, _I, _D, _DP], _I),
+    "lemc_tau_binning": ([_DP, _I, _I, _DP, _DP, _DP, _IP], _I),
     "lemc_sweep_device": ([_P, _I, _I, _I, C.c_float, C.c_uint64, C.c_uint32, _I, _I, _D, _I, _I,
                            _I32P, _I, _P, _P, _P, _P], _I),
     "lemc_set_probes": ([_P, _I32P, _I], _I),

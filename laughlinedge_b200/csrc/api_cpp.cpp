@@ -126,59 +126,18 @@ struct Job {
   }
 };
 
-double measure_acceptance(lemc_ctx* ctx, unsigned sweeps) {
-  check(lemc_reset_accumulators(ctx), "lemc_reset_accumulators");
-  check(lemc_run(ctx, int(std::max(1u, sweeps)), 0), "lemc_run");
-  lemc_stats st;
-  check(lemc_read_stats(ctx, &st), "lemc_read_stats");
-  return st.acceptance;
-}
-
-// Secant/bisection search of the Gaussian step for the target acceptance,
-// bounded in iterations (reference em_bisection.cu:49-153).
+// Step search for the target acceptance, bounded in iterations (reference
+// em_bisection.cu:49-153): lemc_tune_step on the live chain.
 void optimal_step(lemc_ctx* ctx, edgeMC::monteCarloParameters& p) {
   if (!(p.acceptance_tol < 1.0f)) return;
-  auto acc_at = [&](float s) {
-    check(lemc_set_step(ctx, s), "lemc_set_step");
-    return measure_acceptance(ctx, p.targetAcceptanceMoves);
-  };
-  const double tgt = p.targetAcceptance, tol = p.acceptance_tol;
-  float s2 = p.randomStep;
-  double a2 = acc_at(s2);
-  if (std::fabs(a2 - tgt) < tol) return;
-  float s1 = s2;
-  double a1 = a2;
-  for (int it = 0; it < 40 && (a2 - tgt) * (a1 - tgt) > 0; ++it) {
-    s1 *= (a2 > tgt) ? 2.0f : 0.5f;
-    a1 = acc_at(s1);
-  }
-  if (std::fabs(a1 - tgt) < tol) {
-    p.randomStep = s1;
-    check(lemc_set_step(ctx, s1), "lemc_set_step");
-    return;
-  }
-  if (s2 < s1) {
-    std::swap(s1, s2);
-    std::swap(a1, a2);
-  }
-  for (int it = 0; it < 60; ++it) {
-    const float g = float(((tgt - a1) * s2 + (a2 - tgt) * s1) / (a2 - a1));
-    const double ag = acc_at(g);
-    if (std::fabs(ag - tgt) < tol) {
-      p.randomStep = g;
-      return;
-    }
-    if ((ag - tgt) * (a1 - tgt) < 0) {
-      a2 = ag;
-      s2 = g;
-    } else if ((ag - tgt) * (a2 - tgt) < 0) {
-      a1 = ag;
-      s1 = g;
-    } else {
-      break;
-    }
-  }
-  die("\nSomething went wrong with the bisection search for the optimal Markov-Chain step\nCheck the code");
+  check(lemc_set_step(ctx, p.randomStep), "lemc_set_step");
+  float sigma = p.randomStep;
+  const int st = lemc_tune_step(ctx, p.targetAcceptance, p.acceptance_tol,
+                                int(std::max(1u, p.targetAcceptanceMoves)), &sigma, nullptr);
+  if (st == LEMC_ERR_NUMERIC)
+    die("\nSomething went wrong with the bisection search for the optimal Markov-Chain step\nCheck the code");
+  check(st, "lemc_tune_step");
+  p.randomStep = sigma;
 }
 
 int default_precision(const Job& j, unsigned walkers) {

@@ -72,15 +72,18 @@ struct DevBuf {
 
 // Sokal's automatic windowing estimate of the integrated autocorrelation time
 // of one series (A. D. Sokal, "Monte Carlo methods in statistical mechanics",
-// 1997): tau(M) = 1/2 + sum_{t=1..M} rho(t), smallest M with M >= c tau(M).
-double tau_int_sokal(const std::vector<double>& x, double c = 5.0) {
-  const size_t T = x.size();
+// 1997): tau(M) = 1/2 + sum_{t=1..M} rho(t), smallest window M with
+// M >= c tau(M).  NaN when no window up to T/2 satisfies the condition, when
+// the series is shorter than 100 or than 50 max(tau, 1) (below that the estimate is biased low by
+// the subtracted sample mean and a self-consistent window can appear
+// spuriously), or when the series is constant.
+double tau_int_sokal(const double* x, size_t T, double c = 5.0) {
   if (T < 8) return NAN;
   double mean = 0;
-  for (double v : x) mean += v;
+  for (size_t i = 0; i < T; ++i) mean += x[i];
   mean /= T;
   double c0 = 0;
-  for (double v : x) c0 += (v - mean) * (v - mean);
+  for (size_t i = 0; i < T; ++i) c0 += (x[i] - mean) * (x[i] - mean);
   c0 /= T;
   if (!(c0 > 0)) return NAN;
   double tau = 0.5;
@@ -89,9 +92,55 @@ double tau_int_sokal(const std::vector<double>& x, double c = 5.0) {
     for (size_t s = 0; s + t < T; ++s) ct += (x[s] - mean) * (x[s + t] - mean);
     ct /= T;
     tau += ct / c0;
-    if (double(t) >= c * tau) return tau;
+    if (double(t) >= c * tau) return (T >= 100 && double(T) >= 50.0 * std::max(tau, 1.0)) ? tau : NAN;
   }
-  return tau;
+  return NAN;
+}
+
+// Binning analysis (H. Flyvbjerg and H. G. Petersen, J. Chem. Phys. 91, 461
+// (1989)): at bin length b = 2^k the variance of the bin means s_b^2 gives
+// tau(b) = b s_b^2 / (2 s_1^2), which rises to the integrated autocorrelation
+// time once b is well above it.  Levels run while at least min_bins bins
+// remain; the estimate is the last level, its error tau(b) sqrt(2 / (n_b - 1)),
+// and the plateau is declared when the last two levels agree within twice
+// that error (or 5 %).
+int binning(const double* x, size_t T, int min_bins, double* tau, double* tau_err,
+            double* err_of_mean, int* converged) {
+  if (T < size_t(2 * std::max(2, min_bins))) return LEMC_ERR_ARG;
+  double mean = 0;
+  for (size_t i = 0; i < T; ++i) mean += x[i];
+  mean /= T;
+  double v1 = 0;
+  for (size_t i = 0; i < T; ++i) v1 += (x[i] - mean) * (x[i] - mean);
+  v1 /= double(T - 1);
+  double prev = NAN, last = NAN, last_err = NAN, last_em = NAN;
+  for (size_t b = 1;; b *= 2) {
+    const size_t nb = T / b;
+    if (nb < size_t(std::max(2, min_bins))) break;
+    double mb = 0;
+    std::vector<double> means(nb);
+    for (size_t j = 0; j < nb; ++j) {
+      double sm = 0;
+      for (size_t i = 0; i < b; ++i) sm += x[j * b + i];
+      means[j] = sm / b;
+      mb += means[j];
+    }
+    mb /= nb;
+    double sb = 0;
+    for (double m : means) sb += (m - mb) * (m - mb);
+    sb /= double(nb - 1);
+    prev = last;
+    last = v1 > 0 ? 0.5 * b * sb / v1 : NAN;
+    last_err = last * std::sqrt(2.0 / double(nb - 1));
+    last_em = std::sqrt(sb / nb);
+  }
+  if (tau) *tau = last;
+  if (tau_err) *tau_err = last_err;
+  if (err_of_mean) *err_of_mean = last_em;
+  if (converged)
+    *converged = (std::isfinite(prev) && std::isfinite(last) &&
+                  std::fabs(last - prev) <= std::max(2.0 * last_err, 0.05 * last)) ? 1 : 0;
+  return LEMC_OK;
 }
 
 }  // namespace
@@ -1067,19 +1116,22 @@ int lemc_read_stats(lemc_ctx* c, lemc_stats* st) {
   st->sweeps = c->sweeps;
   st->measurements = c->meas;
   st->acceptance = swept > 0 ? tot / (swept * c->W * c->N) : 0.0;
+  // tau_int: Sokal windowing on the walker-mean series of Re and Im p_k; NaN
+  // (for that k, and then for the maximum) when the series is too short for a
+  // self-consistent window.
   const size_t M = c->host_series.size() / 8;
-  double tmax = NAN;
+  double tmax = 0;
   for (int k = 0; k < 4; ++k) {
     double tk = 0;
     for (int comp = 0; comp < 2; ++comp) {
       std::vector<double> x(M);
       for (size_t i = 0; i < M; ++i) x[i] = c->host_series[8 * i + 2 * k + comp];
-      tk += 0.5 * tau_int_sokal(x);
+      tk += 0.5 * tau_int_sokal(x.data(), x.size());
     }
     st->tau_int_each[k] = tk;
-    if (!std::isnan(tk) && (std::isnan(tmax) || tk > tmax)) tmax = tk;
+    tmax = (std::isnan(tk) || std::isnan(tmax)) ? NAN : std::max(tmax, tk);
   }
-  st->tau_int = tmax;
+  st->tau_int = M > 0 ? tmax : NAN;
   st->ms_sweep = c->ms_sweep;
   st->ms_basis = c->ms_basis;
   st->ms_gram = c->ms_gram;
@@ -1167,6 +1219,75 @@ int lemc_gram_device(lemc_ctx* c, const void* V, const void* rec_w, int W, int l
   LEMC_CUDA(cudaEventRecord(c->ev[3], c->stream));
   LEMC_CUDA(cudaStreamWaitEvent(user, c->ev[3], 0));
   return LEMC_OK;
+}
+
+// Acceptance of the current step over `moves` unmeasured sweeps of the live
+// chain (the walkers advance; the accumulators are reset).
+static int acceptance_at(lemc_ctx* c, float sigma, int moves, double* acc) {
+  LEMC_TRY(lemc_set_step(c, sigma));
+  LEMC_TRY(lemc_reset_accumulators(c));
+  LEMC_TRY(lemc_run(c, moves, 0));
+  lemc_stats st;
+  LEMC_TRY(lemc_read_stats(c, &st));
+  *acc = st.acceptance;
+  return LEMC_OK;
+}
+
+int lemc_tune_step(lemc_ctx* c, double target, double tol, int moves, float* sigma,
+                   double* acceptance) {
+  if (!c || !(target > 0 && target < 1) || !(tol > 0) || moves <= 0) return LEMC_ERR_ARG;
+  if (!c->walkers_ready) return LEMC_ERR_STATE;
+  float s2 = c->cfg.step_sigma;
+  double a2 = 0;
+  LEMC_TRY(acceptance_at(c, s2, moves, &a2));
+  auto done = [&](float s, double a) {
+    if (sigma) *sigma = s;
+    if (acceptance) *acceptance = a;
+    return lemc_set_step(c, s);
+  };
+  if (std::fabs(a2 - target) < tol) return done(s2, a2);
+  // bracket: double (acceptance too high) or halve the step until it crosses
+  float s1 = s2;
+  double a1 = a2;
+  for (int it = 0; it < 40 && (a2 - target) * (a1 - target) > 0; ++it) {
+    s1 *= (a2 > target) ? 2.0f : 0.5f;
+    LEMC_TRY(acceptance_at(c, s1, moves, &a1));
+  }
+  if (std::fabs(a1 - target) < tol) return done(s1, a1);
+  if ((a2 - target) * (a1 - target) > 0) return LEMC_ERR_NUMERIC;
+  if (s2 < s1) {
+    std::swap(s1, s2);
+    std::swap(a1, a2);
+  }
+  // regula falsi on the bracket [s1, s2]
+  for (int it = 0; it < 60; ++it) {
+    const float g = float(((target - a1) * s2 + (a2 - target) * s1) / (a2 - a1));
+    double ag = 0;
+    LEMC_TRY(acceptance_at(c, g, moves, &ag));
+    if (std::fabs(ag - target) < tol) return done(g, ag);
+    if ((ag - target) * (a1 - target) < 0) {
+      a2 = ag;
+      s2 = g;
+    } else if ((ag - target) * (a2 - target) < 0) {
+      a1 = ag;
+      s1 = g;
+    } else {
+      break;
+    }
+  }
+  return LEMC_ERR_NUMERIC;
+}
+
+int lemc_tau_sokal(const double* x, int T, double c, double* tau) {
+  if (!x || T < 0 || !tau) return LEMC_ERR_ARG;
+  *tau = tau_int_sokal(x, size_t(T), c > 0 ? c : 5.0);
+  return LEMC_OK;
+}
+
+int lemc_tau_binning(const double* x, int T, int min_bins, double* tau, double* tau_err,
+                     double* err_of_mean, int* converged) {
+  if (!x || T < 0) return LEMC_ERR_ARG;
+  return binning(x, size_t(T), min_bins > 0 ? min_bins : 16, tau, tau_err, err_of_mean, converged);
 }
 
 }  // extern "C"

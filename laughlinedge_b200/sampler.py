@@ -141,6 +141,39 @@ def occupation(particles, inverse_filling, dL, l_cutoff, n_walkers, sweeps, burn
     return out.view(np.complex128).reshape(D, D, l_cutoff), acc.value
 
 
+def tau_sokal(x, c: float = 5.0) -> float:
+    """Sokal windowed integrated autocorrelation time of a series (NaN when the
+    series is too short for a self-consistent window)."""
+    a = np.ascontiguousarray(x, dtype=np.float64)
+    t = C.c_double()
+    check(_lib.load().lemc_tau_sokal(dptr(a), len(a), c, C.byref(t)), "lemc_tau_sokal")
+    return t.value
+
+
+def tau_binning(x, min_bins: int = 16):
+    """Binning analysis of a series: (tau, tau_err, error of the mean, converged)."""
+    a = np.ascontiguousarray(x, dtype=np.float64)
+    t, te, em, cv = C.c_double(), C.c_double(), C.c_double(), C.c_int()
+    check(_lib.load().lemc_tau_binning(dptr(a), len(a), min_bins, C.byref(t), C.byref(te),
+                                       C.byref(em), C.byref(cv)), "lemc_tau_binning")
+    return t.value, te.value, em.value, bool(cv.value)
+
+
+def series_tau(series: np.ndarray):
+    """tau_int of p_1..p_4 from a walker-mean series [T, 8] (Re/Im per k): per k
+    the mean of the Re and Im estimates, Sokal and binning; the max over k."""
+    sok, binn, conv = [], [], True
+    for k in range(4):
+        s = [tau_sokal(series[:, 2 * k + c]) for c in range(2)]
+        b = [tau_binning(series[:, 2 * k + c]) for c in range(2)]
+        sok.append(0.5 * (s[0] + s[1]))
+        binn.append(0.5 * (b[0][0] + b[1][0]))
+        conv = conv and b[0][3] and b[1][3]
+    return {"sokal": float(max(sok)), "sokal_each": [float(v) for v in sok],
+            "binning": float(max(binn)), "binning_each": [float(v) for v in binn],
+            "binning_plateau": bool(conv), "series_length": int(series.shape[0])}
+
+
 @dataclass
 class SamplerConfig:
     particles: int
@@ -221,6 +254,16 @@ class Sampler:
                 return -1
         self._hook = _lib.STEP_HOOK(_cb)
         check(self.lib.lemc_run_hooked(self._h, int(n_sweeps), self._hook, None), "lemc_run_hooked")
+
+    def set_step(self, sigma: float):
+        check(self.lib.lemc_set_step(self._h, float(sigma)), "lemc_set_step")
+
+    def tune_step(self, target: float = 0.5, tol: float = 0.01, moves: int = 100):
+        """Tune the Gaussian step on the live chain; returns (sigma, acceptance)."""
+        sg, acc = C.c_float(), C.c_double()
+        check(self.lib.lemc_tune_step(self._h, target, tol, moves, C.byref(sg), C.byref(acc)),
+              "lemc_tune_step")
+        return sg.value, acc.value
 
     def reset(self):
         check(self.lib.lemc_reset_accumulators(self._h), "lemc_reset_accumulators")
