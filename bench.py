@@ -618,6 +618,77 @@ def run_batched(args, rank, local):
     print(json.dumps(line), flush=True)
 
 
+EVOLUTION = {
+    "workload": "time_evolution_m3_N100_dL0-16even_W65536",
+    "particles": 100, "inverse_filling": 3, "omega": 2e-3, "kappa": 2e-5,
+    "sectors": list(range(0, 17, 2)), "k": 2, "eps": 1e-3, "t0": 50.0, "tau": 10.0,
+    "walkers": 65536, "sigma": 0.3, "seed": 42, "dt": 0.05, "steps": 4000, "n_theta": 256,
+    "burn": 1000, "sweeps": 200, "train_configs": 1 << 20, "train_steps": 5000,
+}
+
+
+def run_evolution(args, rank, local):
+    """Time-evolution pipeline: the DeepSets proposal trained on the plain
+    chain; matrix elements of sectors {0, 2, ..., 16} (526 states) under the
+    drive r^2 cos(2 theta) with the learned proposal and the TF32x3
+    contraction; FP64 RK4 evolution of 4000 steps of dt = 0.05 in the
+    S-orthonormal basis on the GPU; delta rho(theta, t) on 256 angles.  Each
+    stage timed on the host clock after a device synchronisation."""
+    if rank != 0:
+        return
+    import numpy as np
+    import torch
+
+    import laughlinedge_b200 as L
+    w = EVOLUTION
+    torch.cuda.set_device(local)
+    N, m, W = w["particles"], w["inverse_filling"], w["walkers"]
+    t_all = time.perf_counter()
+    p0 = L.Sampler(L.SamplerConfig(N, m, W, step_sigma=w["sigma"], seed=w["seed"], lanes_per_walker=-1),
+                   [1, 2, 3, 4])
+    p0.init_walkers()
+    p0.run(w["burn"], measure=False)
+    n_snap = w["train_configs"] // W
+    buf = torch.empty((n_snap * W, N, 2), dtype=torch.float32, device="cuda")
+    for k in range(n_snap):
+        p0.run(10, measure=False)
+        p0.copy_positions_device(buf[k * W:(k + 1) * W].data_ptr())
+    start_xy = p0.positions()
+    p0.close()
+    prop = L.LearnedProposal(N, m, init_sigma=w["sigma"], seed=w["seed"])
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    prop.train(buf.data_ptr(), buf.shape[0], steps=w["train_steps"], batch=1024, pairs=32, lr=3e-3,
+               es_sigma=0.02, seed=w["seed"])
+    t_train = time.perf_counter() - t0
+    del buf
+    prof = lambda t: w["eps"] * math.exp(-((t - w["t0"]) ** 2) / (2 * w["tau"] ** 2))
+    out = L.edge_response(N, m, w["sectors"], w["k"], w["omega"], w["kappa"], prof,
+                          end_time=w["steps"] * w["dt"], save_step=w["dt"], n_walkers=W, burn_in=100,
+                          sweeps=w["sweeps"], step_sigma=w["sigma"], seed=w["seed"] + 1,
+                          gram_mode=L._lib.GRAM_TF32X3, proposal=prop, substeps=1,
+                          n_theta=w["n_theta"], init_xy=start_xy, graph_batch=args.graph_batch)
+    prop.close()
+    dens = out["density"]
+    rho_t = out["rho_t"]
+    D = out["M"].shape[0]
+    line = {"metric": "edge_density_response_pipeline_s", "value": sum(out["timings"].values()),
+            "unit": "s", "workload": w["workload"], "n_gpus": 1, "higher_is_better": False,
+            "data": "synthetic", "dtype": "f32+bf16-net+tf32x3 sampling, f64 evolution",
+            "config": {k: w[k] for k in w if k != "sectors"}, "basis_states": D,
+            "timings_s": dict(out["timings"], train_proposal_s=t_train),
+            "sampling_walker_sweeps_per_s": W * (w["sweeps"] + 100) / out["timings"]["sampling_s"],
+            "evolution_steps_per_s": w["steps"] / out["timings"]["evolution_s"],
+            "acceptance": out["acceptance"], "rank": out["rank"],
+            "norm_drift": float(np.max(np.abs(out["norms"] - 1.0))),
+            "max_abs_delta_rho": float(np.max(np.abs(dens))),
+            "max_abs_delta_rho_l": [float(np.max(np.abs(rho_t[:, q] - rho_t[0, q])))
+                                   for q in range(rho_t.shape[1])],
+            "n_times": int(dens.shape[0]), "n_theta": int(dens.shape[1]),
+            "total_wall_s": time.perf_counter() - t_all}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)

@@ -160,6 +160,15 @@ LEMC_API int lemc_set_guide_rows(lemc_ctx* ctx, const int32_t* rows, int n_rows)
  * (edge density Fourier components, reference em_edgeResponse.tpp:136-163,
  * and the dynamic structure factor, em_dsf.cu:101-117). */
 LEMC_API int lemc_set_probes(lemc_ctx* ctx, const int32_t* l, int n);
+/* Built-in excitation potential for the USER weight plane, in place of a hook:
+ * U(z) = amplitude * sum_i r_i^k cos(k theta_i) = amplitude * Re sum_i z_i^k,
+ * formed on the device from the recorded power sums at every measured sweep
+ * (k <= the basis' largest degree; k = 0 switches it off).  The cross-sector
+ * sums of lemc_read_cross then hold <f|U|g>.  This is the multipole drive
+ * delta V = eps r^k cos(k theta) f(t) of the edge-response pipeline (the
+ * reference's excitationResponse_compute with such a lambda,
+ * em_edgeResponse.tpp:26-194); the temporal profile f enters the evolution. */
+LEMC_API int lemc_set_multipole_potential(lemc_ctx* ctx, int k, double amplitude);
 /* Initial walker positions; host_xy == NULL draws them uniformly in the
  * init disk from the Philox stream (replaces particle_positions_initialize,
  * modules/edge_mc/em_markovchain.cu:223-263). */
@@ -196,6 +205,11 @@ LEMC_API int lemc_total_dim(const lemc_ctx* ctx, int* dim);
  *   H4[a][b] = sum_samples w1 * (sum_i |z_i|^4) conj(v_a) v_b
  * with v_a = prod_j p_{lambda_j}, p_k = sum_i (z_i / R)^k.  Any output may be
  * NULL.  *n_samples receives the number of accumulated samples.
+ * Range: the device holds each state's values times a range factor c_a (the
+ * inverse geometric mean of |v_a| over the walkers at the first measured sweep
+ * of the basis, Laughlin guide), so that FP32 values and accumulations stay
+ * O(1) in every sector; the sums returned here are divided by c_a c_b.  A
+ * non-finite sum is returned with LEMC_ERR_NUMERIC (outputs still written).
  * Replaces the device->host copy and block averaging of em_spectrum.cu:256-359. */
 LEMC_API int lemc_read_gram(lemc_ctx* ctx, int sector_index, double* S, double* H2,
                    double* H4, double* n_samples);
@@ -204,7 +218,8 @@ LEMC_API int lemc_read_gram(lemc_ctx* ctx, int sector_index, double* S, double* 
  *   Ccos[a][b]  = sum w1 (sum_i cos l theta_i) conj(v_a) v_b,
  *   Csin[a][b]  = sum w1 (sum_i sin l theta_i) conj(v_a) v_b,
  * l = |dL_b - dL_a|; Ccos/Csin are zero unless l is a probe.  Any output may
- * be NULL.  Used by the dynamic structure factor (em_dsf.cu:18-158) and the
+ * be NULL.  Range factors are undone and non-finite sums reported as in
+ * lemc_read_gram.  Used by the dynamic structure factor (em_dsf.cu:18-158) and the
  * excitation response (em_edgeResponse.tpp:26-194). */
 LEMC_API int lemc_read_cross(lemc_ctx* ctx, int sector_a, int sector_b, double* Cuser,
                              double* Ccos, double* Csin);
@@ -222,6 +237,29 @@ LEMC_API int lemc_read_stats(lemc_ctx* ctx, lemc_stats* st);
 LEMC_API int lemc_read_positions(lemc_ctx* ctx, float* host_xy);
 /* Walker-mean series of Re/Im p_1..p_4 per measurement: series[m*8 + 2(k-1) + c]. */
 LEMC_API int lemc_read_series(lemc_ctx* ctx, double* series, int max_meas, int* n_meas);
+
+/* ---- bins and jackknife error bars -------------------------------------------
+ * The reference leaves error bars to repetitions of whole runs, each saved as
+ * a numbered .tsv (main.cu:18-20, em_spectrum.cu:393-414).  Here one run is cut
+ * into bins: lemc_close_bin ends the current bin at the measurements made
+ * since the previous close (LEMC_GUIDE_LAUGHLIN; a bin must hold at least one
+ * measurement, and should span many autocorrelation times).  Bins are kept on
+ * the host (3 D_s^2 complex FP64 per sector each) until
+ * lemc_reset_accumulators. */
+LEMC_API int lemc_close_bin(lemc_ctx* ctx);
+LEMC_API int lemc_n_bins(const lemc_ctx* ctx, int* n_bins);
+/* Raw Gram sums of one bin and sector, as lemc_read_gram. */
+LEMC_API int lemc_read_gram_bin(lemc_ctx* ctx, int bin, int sector_index, double* S, double* H2,
+                                double* H4, double* n_samples);
+/* Jackknife (leave one bin out) over n_bins bins of raw Gram sums of one
+ * sector (S, H2, H4: [n_bins][D][D] complex, interleaved): evals of the full
+ * sums (normalised as lemc_normalise, solved as lemc_geneig) and their
+ * standard errors; M_err, H_err (D x D real, may be NULL) the errors of the
+ * normalised matrix entries (modulus of the complex deviation).  Host only. */
+LEMC_API int lemc_jackknife_spectrum(int D, int n_bins, const double* S, const double* H2,
+                                     const double* H4, double omega, double kappa, double eps,
+                                     double* evals, double* evals_err, double* M_err,
+                                     double* H_err);
 
 /* ---- error analysis of a scalar Monte Carlo series (host only) -------------
  * The reference leaves error bars to post-processing of repeated runs
@@ -379,6 +417,19 @@ LEMC_API int lemc_occupation_static(const lemc_occupation_config* cfg, double* o
 LEMC_API int lemc_geneig(int D, const double* H, const double* M, double eps,
                 double* evals, double* evecs, int* rank);
 
+/* Edge dynamic structure factor from the normalised matrices of the sectors
+ * {0, dL} (D = 1 + D_dL, row 0 the Laughlin state; complex D x D, interleaved):
+ * the generalized problem of the dL block, H[1:,1:] c = E M[1:,1:] c with
+ * c^H M c = 1 (eigenvalues ascending), and the weight of mode j,
+ * |sum_a (Vc - i Vs)[0][a+1] c_j[a]|^2 (Vc, Vs: the cos / sin(dL theta)
+ * excitation matrices).  energies and weights receive D - 1 entries, *n_modes
+ * the kept rank (weights beyond it NaN).  Replaces
+ * ges::generalizedEigenproblem::extract_dsf_coefficients
+ * (modules/eigensolver/generalized_eigenproblem.cpp:54-95). */
+LEMC_API int lemc_dsf_weights(int D, const double* H, const double* M, const double* Vc,
+                              const double* Vs, double eps, double* energies, double* weights,
+                              int* n_modes);
+
 /* Generalized spectra of one sector for n confinement strengths, computed on
  * the GPU in FP64 (the kappa sweep of the batched form).  S, H2, H4 are the raw
  * Gram sums of lemc_read_gram (D x D complex, interleaved); for each j the
@@ -427,6 +478,18 @@ LEMC_API int lemc_evolve_device(int D, const double* M, const double* H, const d
                                 int L, const double* rho, lemc_profile_fn f, void* user,
                                 double end_time, double save_step, int substeps, double eps,
                                 double* out, double* norms, int* n_save, int* rank);
+
+/* Edge density response on an angular grid, from the Fourier components
+ * <rho_l>(t) = C^H rho_l C of the evolution (rho_t: [n_times][L] complex,
+ * interleaved, angular momenta l[q] >= 0):
+ *   out[t][g] = (1/2pi) [ d_0 + 2 Re sum_{l>0} e^{-i l theta_g} d_l(t) ],
+ *   d_l(t) = <rho_l>(t) - rho_ref[l], theta_g = 2 pi g / n_theta,
+ * rho_ref (L complex) NULL selects rho_t[0] (the response to the drive).
+ * Computed on the GPU in FP64.  Completes the reference's
+ * edgeDensityResponse_compute, which stops at the components
+ * (modules/dynamics/dynamics.cpp:110-125, :293-306). */
+LEMC_API int lemc_edge_density_grid(int L, const int32_t* l, int n_times, const double* rho_t,
+                                    const double* rho_ref, int n_theta, double* out);
 
 #ifdef __cplusplus
 }

@@ -3,11 +3,15 @@
 The compute path is the native library ``liblemc.so`` (hand-written CUDA for
 sm_100a behind the C-ABI of include/lemc.h); this package only binds it.
 """
-from . import _lib
+from . import _lib, dynamics
 from ._lib import LemcError, load
+from .dynamics import density_grid, edge_response
 from .proposal import LearnedProposal
-from .sampler import (Sampler, SamplerConfig, evolve, evolve_device, geneig, geneig_sweep, normalise,
-                      partitions)
+from .sampler import (Sampler, SamplerConfig, dsf_compute, dsf_weights, evolve, evolve_device, geneig,
+                      geneig_sweep, jackknife_spectrum, normalise, partitions, series_tau, tau_binning,
+                      tau_sokal)
 
-__all__ = ["LearnedProposal", "LemcError", "Sampler", "SamplerConfig", "evolve", "evolve_device", "geneig", "geneig_sweep", "load",
-           "normalise", "partitions", "_lib"]
+__all__ = ["LearnedProposal", "LemcError", "Sampler", "SamplerConfig", "density_grid", "dsf_compute",
+           "dsf_weights", "edge_response", "evolve",
+           "evolve_device", "geneig", "geneig_sweep", "jackknife_spectrum", "load", "normalise", "partitions", "series_tau",
+           "tau_binning", "tau_sokal", "_lib"]

@@ -105,6 +105,10 @@ _SIGNATURES = {
     "lemc_read_positions": ([_P, _FP], _I),
     "lemc_read_series": ([_P, _DP, _I, _IP], _I),
     "lemc_tau_sokal": ([_DP, _I, _D, _DP], _I),
+    "lemc_close_bin": ([_P], _I),
+    "lemc_n_bins": ([_P, _IP], _I),
+    "lemc_read_gram_bin": ([_P, _I, _I, _DP, _DP, _DP, _DP], _I),
+    "lemc_jackknife_spectrum": ([_I, _I, _DP, _DP, _DP, _D, _D, _D, _DP, _DP, _DP, _DP], _I),
     "lemc_tau_binning": ([_DP, _I, _I, _DP, _DP, _DP, _IP], _I),
     "lemc_sweep_device": ([_P, _I, _I, _I, C.c_float, C.c_uint64, C.c_uint32, _I, _I, _D, _I, _I,
                            _I32P, _I, _P, _P, _P, _P], _I),
@@ -113,6 +117,7 @@ _SIGNATURES = {
     "lemc_basis_device": ([_P, _P, _I, _P, _I, _P], _I),
     "lemc_gram_device": ([_P, _P, _P, _I, _I, _I, _P], _I),
     "lemc_geneig": ([_I, _DP, _DP, _D, _DP, _DP, _IP], _I),
+    "lemc_dsf_weights": ([_I, _DP, _DP, _DP, _DP, _D, _DP, _DP, _IP], _I),
     "lemc_proposal_n_params": ([_IP], _I),
     "lemc_proposal_create": ([_I, _I, C.c_float, C.c_uint64, C.POINTER(_P)], _I),
     "lemc_proposal_destroy": ([_P], _I),
@@ -124,6 +129,8 @@ _SIGNATURES = {
     "lemc_copy_positions_device": ([_P, _P], _I),
     "lemc_geneig_sweep": ([_I, _DP, _DP, _DP, _DP, _DP, _I, _D, _DP, _IP], _I),
     "lemc_normalise": ([_I, _DP, _DP, _DP, _D, _D, _DP, _DP], _I),
+    "lemc_edge_density_grid": ([_I, _I32P, _I, _DP, _DP, _I, _DP], _I),
+    "lemc_set_multipole_potential": ([_P, _I, _D], _I),
     "lemc_evolve": ([_I, _DP, _DP, _DP, _I, _DP, PROFILE_FN, _P, _D, _D, _DP, _DP, _IP], _I),
     "lemc_evolve_device": ([_I, _DP, _DP, _DP, _I, _DP, PROFILE_FN, _P, _D, _D, _I, _D, _DP, _DP,
                             _IP, _IP], _I),

@@ -354,29 +354,27 @@ std::vector<double> generalizedEigenproblem::extract_spectrum() {
 
 std::vector<std::pair<double, double>> generalizedEigenproblem::extract_dsf_coefficients(
     cmatrix<double>& VC, cmatrix<double>& VS) {
-  const int n = H0_.rows() - 1;
+  const int D = H0_.rows();
   std::vector<std::pair<double, double>> out;
-  if (n <= 0) return out;
-  std::vector<double> h(2 * n * n), m(2 * n * n), ev(n), vec(2 * n * n);
-  for (int a = 0; a < n; ++a)
-    for (int b = 0; b < n; ++b) {
-      const size_t o = 2 * (size_t(a) * n + b);
-      h[o] = re(H0_(a + 1, b + 1));
-      h[o + 1] = im(H0_(a + 1, b + 1));
-      m[o] = re(M0_(a + 1, b + 1));
-      m[o + 1] = im(M0_(a + 1, b + 1));
+  if (D < 2) return out;
+  std::vector<double> h(2 * D * D), m(2 * D * D), vc(2 * D * D), vs(2 * D * D), e(D), w(D);
+  for (int a = 0; a < D; ++a)
+    for (int b = 0; b < D; ++b) {
+      const size_t o = 2 * (size_t(a) * D + b);
+      h[o] = re(H0_(a, b));
+      h[o + 1] = im(H0_(a, b));
+      m[o] = re(M0_(a, b));
+      m[o + 1] = im(M0_(a, b));
+      vc[o] = re(VC(a, b));
+      vc[o + 1] = im(VC(a, b));
+      vs[o] = re(VS(a, b));
+      vs[o + 1] = im(VS(a, b));
     }
   int rank = 0;
-  check(lemc_geneig(n, h.data(), m.data(), 1e-12, ev.data(), vec.data(), &rank), "lemc_geneig");
-  for (int j = 0; j < rank; ++j) {
-    complex<double> me(0.0);
-    for (int a = 0; a < n; ++a) {
-      const complex<double> v = VC(0, a + 1) - complex<double>(0.0, 1.0) * VS(0, a + 1);
-      const size_t o = 2 * (size_t(a) * n + j);
-      me += v * complex<double>(vec[o], vec[o + 1]);
-    }
-    out.push_back({ev[j], norm(me)});
-  }
+  check(lemc_dsf_weights(D, h.data(), m.data(), vc.data(), vs.data(), 1e-12, e.data(), w.data(),
+                         &rank),
+        "lemc_dsf_weights");
+  for (int j = 0; j < rank; ++j) out.push_back({e[j], w[j]});
   return out;
 }
 

@@ -14,8 +14,11 @@
 // sits on the thread's stack in shared memory, and that load is also issued
 // one node ahead.  Outputs are written as FP32 planes V[row][w] (Re rows,
 // then Im rows of each sector), walker-contiguous so that consecutive threads
-// write consecutive addresses.  Segment-0 blocks also reduce Re/Im p_1..p_4
-// into the walker-mean series used for the integrated autocorrelation time.
+// write consecutive addresses, each multiplied by its row's range factor when
+// the program carries one (the sampling context sets them so that the values
+// of every state are O(1) on a geometric mean over walkers).  Segment-0 blocks
+// also reduce Re/Im p_1..p_4 into the walker-mean series used for the
+// integrated autocorrelation time.
 #include <cuda_runtime.h>
 
 #include "lemc_internal.h"
@@ -164,8 +167,14 @@ basis_kernel(const float2* __restrict__ rec_p, int W, int K, float pN, BasisProg
     const Vals<P> v = vmul<P>(a, b);
     if (descend) vstore<P>(stk + nd.x * R, v);
     if (nd.z >= 0) {
-      row_store<P>(Vw + (size_t)nd.z * ldv, v, false);
-      row_store<P>(Vw + (size_t)nd.w * ldv, v, true);
+      Vals<P> out = v;
+      if (prog.row_scale) {
+        const float sc = __ldg(prog.row_scale + nd.z);
+#pragma unroll
+        for (int i = 0; i < P; ++i) out.c[i] = make_float2(sc * v.c[i].x, sc * v.c[i].y);
+      }
+      row_store<P>(Vw + (size_t)nd.z * ldv, out, false);
+      row_store<P>(Vw + (size_t)nd.w * ldv, out, true);
     }
     ax = descend ? v : an;
   };
@@ -197,7 +206,22 @@ int launch_p(const float2* rec_p, int W, int K, int N, const BasisProgram& prog,
   return cudaPeekAtLastError() == cudaSuccess ? LEMC_OK : LEMC_ERR_CUDA;
 }
 
+// USER plane of a multipole potential U = amp sum_i r_i^k cos(k theta_i)
+// = amp R^k Re p_k, from the recorded (z/R)^k power sums.
+__global__ void multipole_plane_kernel(const float2* __restrict__ rec_p, int W, int k, float scale,
+                                       float* __restrict__ plane) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w < W) plane[w] = scale * rec_p[size_t(k - 1) * W + w].x;
+}
+
 }  // namespace
+
+int launch_multipole_plane(const float2* rec_p, int W, int K, int k, double scale, float* plane,
+                           cudaStream_t st) {
+  if (k < 1 || k > K || W <= 0) return LEMC_ERR_ARG;
+  multipole_plane_kernel<<<(W + 255) / 256, 256, 0, st>>>(rec_p, W, k, float(scale), plane);
+  return cudaPeekAtLastError() == cudaSuccess ? LEMC_OK : LEMC_ERR_CUDA;
+}
 
 int launch_basis(const float2* rec_p, int W, int K, int N, const BasisProgram& prog, float* V,
                  int ldv, double* series, const uint32_t* series_idx, cudaStream_t st) {

@@ -166,6 +166,20 @@ struct lemc_ctx {
   size_t cross_plane = 0;
   int n_gram_jobs = 0, n_cross_jobs = 0;
   std::vector<int> row_vre, row_vim;  // V rows of each basis row
+  // Range factors: V holds c_r v_r, so the FP32 products and the tensor-core
+  // accumulation of every state stay O(1); the FP64 sums are divided by
+  // c_a c_b when read.  Set once per basis, from the walkers at the first
+  // measured sweep (Laughlin guide; 1 for the row guide, whose ratios v_b/v_a
+  // are formed from V directly).
+  // bins: FP64 Gram sums (device layout, range factors included) of each
+  // closed bin, and the cumulative sums at the last close
+  std::vector<std::vector<double>> bins;
+  std::vector<double> bin_samples;
+  std::vector<double> bin_last;
+  uint64_t bin_last_meas = 0;
+  std::vector<double> row_scale;      // per basis row
+  DevBuf<float> d_row_scale;          // per V row
+  bool scale_pending = false;
 
   std::vector<int> probes;  // angular probes l_q
   // guide rows
@@ -198,6 +212,8 @@ struct lemc_ctx {
 
   bool walkers_ready = false;
   bool hooked = false;  // a user-potential hook fills the USER plane
+  int multipole_k = 0;  // > 0: the USER plane is multipole_amp * sum_i r_i^k cos(k theta_i)
+  double multipole_amp = 0;
   uint64_t sweeps = 0, meas = 0, sweeps_at_reset = 0;
   std::vector<double> host_series;  // [meas][8]
   double ms_sweep = 0, ms_basis = 0, ms_gram = 0;
@@ -465,7 +481,8 @@ int gram_step(lemc_ctx* c, const float* V, const float* rec_w, int ldw, int W, i
                                  int(c->basis.rows.size()), c->D, c->d_row_re.p, c->d_row_im.p,
                                  c->rowacc.p, c->stream);
   }
-  const bool cross = c->n_cross_jobs > 0 && (c->hooked || !c->probes.empty());
+  const bool cross =
+      c->n_cross_jobs > 0 && (c->hooked || c->multipole_k > 0 || !c->probes.empty());
   if (mode == LEMC_GRAM_FP64) {
     const int splits = std::max(1, std::min(64, W / 1024));
     return launch_gram_simt(V, c->Wpad, rec_w, ldw, W, c->jobs.p,
@@ -690,6 +707,7 @@ int lemc_destroy(lemc_ctx* c) {
   c->d_tc_tiles.release();
   c->d_tc_secs.release();
   c->tc_partials.release();
+  c->d_row_scale.release();
   for (auto& e : c->ev)
     if (e) cudaEventDestroy(e);
   for (auto& e : c->pev) cudaEventDestroy(e);
@@ -735,6 +753,15 @@ int lemc_set_sectors(lemc_ctx* c, const int32_t* sectors, int n) {
   LEMC_TRY(c->gram.alloc(6 * c->gram_plane));
   LEMC_TRY(build_program(c));
   LEMC_TRY(alloc_records(c));
+  c->row_scale.assign(c->D, 1.0);
+  LEMC_TRY(c->d_row_scale.alloc(std::max(1, 2 * c->D)));
+  {
+    std::vector<float> ones(std::max(1, 2 * c->D), 1.f);
+    LEMC_CUDA(cudaMemcpy(c->d_row_scale.p, ones.data(), sizeof(float) * ones.size(),
+                         cudaMemcpyHostToDevice));
+  }
+  c->bprog.row_scale = c->d_row_scale.p;
+  c->scale_pending = c->cfg.guide == LEMC_GUIDE_LAUGHLIN;
   c->tc_tiles.clear();
   LEMC_TRY(upload_guide(c));
   return lemc_reset_accumulators(c);
@@ -830,6 +857,10 @@ int lemc_reset_accumulators(lemc_ctx* c) {
     LEMC_CUDA(cudaMemsetAsync(c->tc_partials.p, 0, sizeof(double) * c->tc_partials.n, c->stream));
   if (c->accepted.p) LEMC_CUDA(cudaMemsetAsync(c->accepted.p, 0, 4 * c->W, c->stream));
   c->meas = 0;
+  c->bins.clear();
+  c->bin_samples.clear();
+  c->bin_last.clear();
+  c->bin_last_meas = 0;
   c->host_series.clear();
   c->ms_sweep = c->ms_basis = c->ms_gram = 0;
   c->sweeps_at_reset = c->sweeps;
@@ -887,6 +918,16 @@ int lemc_run_hooked(lemc_ctx* c, int n_sweeps, lemc_step_hook hook, void* user) 
   return run_impl(c, n_sweeps, 1, hook, user);
 }
 
+int lemc_set_multipole_potential(lemc_ctx* c, int k, double amplitude) {
+  if (!c || k < 0) return LEMC_ERR_ARG;
+  if (k > 0 && !c->has_basis) return LEMC_ERR_STATE;
+  if (k > c->K) return LEMC_ERR_CAPACITY;
+  c->multipole_k = k;
+  c->multipole_amp = amplitude;
+  ++c->version;
+  return LEMC_OK;
+}
+
 int lemc_set_probes(lemc_ctx* c, const int32_t* l, int n) {
   if (!c || n < 0 || n > LEMC_MAX_PROBES || (n > 0 && !l)) return LEMC_ERR_ARG;
   ++c->version;
@@ -895,6 +936,13 @@ int lemc_set_probes(lemc_ctx* c, const int32_t* l, int n) {
     if (q < 0 || q > 1024) return LEMC_ERR_ARG;
   if (c->has_basis) LEMC_TRY(build_jobs(c));
   return LEMC_OK;
+}
+
+static int multipole_step(lemc_ctx* c) {
+  if (c->multipole_k <= 0) return LEMC_OK;
+  return launch_multipole_plane(c->rec_p.p, c->W, c->K, c->multipole_k,
+                                c->multipole_amp * std::pow(double(c->R), c->multipole_k),
+                                c->rec_w.p + size_t(LEMC_W_USER) * c->Wpad, c->stream);
 }
 
 // One measured sweep with every per-step value taken from the device counters
@@ -907,6 +955,7 @@ static int graph_step(lemc_ctx* c) {
   LEMC_TRY(launch_sweep_for(c, a));
   LEMC_TRY(launch_basis(c->rec_p.p, c->W, c->K, c->N, c->bprog, c->V.p, c->Wpad,
                         c->series.p, c->d_ctr.p + 1, c->stream));
+  LEMC_TRY(multipole_step(c));
   LEMC_TRY(gram_step(c, c->V.p, c->rec_w.p, c->Wpad, c->W, c->cfg.gram_mode));
   return launch_advance_counters(c->d_ctr.p, c->stream);
 }
@@ -947,6 +996,55 @@ static int ensure_graph(lemc_ctx* c, int G) {
   return LEMC_OK;
 }
 
+// Range factors c_r = exp(-<ln|v_r|>), the inverse geometric mean of |v_r| over
+// up to 2048 of the current walkers (p_k from their positions in FP64, p_0 = N,
+// ln|p| floored at -80), clamped to [1e-30, 1e30].  Called once per basis
+// before its first measured sweep, with the accumulators empty.
+static int compute_row_scales(lemc_ctx* c) {
+  const int Ws = std::min(c->W, 2048), N = c->N, K = c->K, D = c->D;
+  std::vector<float2> xy(size_t(Ws) * N);
+  LEMC_CUDA(cudaMemcpyAsync(xy.data(), c->pos.p, sizeof(float2) * xy.size(), cudaMemcpyDeviceToHost,
+                            c->stream));
+  LEMC_CUDA(cudaStreamSynchronize(c->stream));
+  std::vector<double> lp(size_t(K + 1) * Ws);  // ln|p_k| per walker
+  const double invR = 1.0 / c->R;
+  for (int w = 0; w < Ws; ++w) {
+    std::vector<double> re(K + 1, 0.0), im(K + 1, 0.0);
+    for (int i = 0; i < N; ++i) {
+      const double x = xy[size_t(w) * N + i].x * invR, y = xy[size_t(w) * N + i].y * invR;
+      double zr = 1, zi = 0;
+      for (int k = 1; k <= K; ++k) {
+        const double t = zr * x - zi * y;
+        zi = zr * y + zi * x;
+        zr = t;
+        re[k] += zr;
+        im[k] += zi;
+      }
+    }
+    lp[w] = std::log(double(N));
+    for (int k = 1; k <= K; ++k)
+      lp[size_t(k) * Ws + w] = std::max(-80.0, 0.5 * std::log(re[k] * re[k] + im[k] * im[k]));
+  }
+  std::vector<float> dev(2 * size_t(D), 1.f);
+  for (int r = 0; r < D; ++r) {
+    double mean = 0;
+    for (const auto& pp : c->basis.rows[r].pairs) {
+      double sk = 0;
+      for (int w = 0; w < Ws; ++w) sk += lp[size_t(pp.part) * Ws + w];
+      mean += pp.mult * sk / Ws;
+    }
+    const double sc = std::min(1e30, std::max(1e-30, std::exp(-mean)));
+    const float scf = float(sc);
+    c->row_scale[r] = double(scf);  // the factor the kernel applies, exactly
+    dev[c->row_vre[r]] = scf;
+    dev[c->row_vim[r]] = scf;
+  }
+  LEMC_CUDA(cudaMemcpyAsync(c->d_row_scale.p, dev.data(), sizeof(float) * dev.size(),
+                            cudaMemcpyHostToDevice, c->stream));
+  LEMC_CUDA(cudaStreamSynchronize(c->stream));
+  return LEMC_OK;
+}
+
 static int run_impl(lemc_ctx* c, int n_sweeps, int measure, lemc_step_hook hook, void* user) {
   if (!c || n_sweeps < 0) return LEMC_ERR_ARG;
   if (!c->walkers_ready) return LEMC_ERR_STATE;
@@ -961,6 +1059,10 @@ static int run_impl(lemc_ctx* c, int n_sweeps, int measure, lemc_step_hook hook,
       done += chunk;
     }
     return LEMC_OK;
+  }
+  if (c->scale_pending && c->meas == 0) {
+    LEMC_TRY(compute_row_scales(c));
+    c->scale_pending = false;
   }
   LEMC_TRY(c->series.alloc(size_t(8) * n_sweeps));
   LEMC_CUDA(cudaMemsetAsync(c->series.p, 0, sizeof(double) * 8 * n_sweeps, c->stream));
@@ -992,6 +1094,7 @@ static int run_impl(lemc_ctx* c, int n_sweeps, int measure, lemc_step_hook hook,
     if (c->profile) LEMC_CUDA(cudaEventRecord(c->pev[4 * s + 1], c->stream));
     LEMC_TRY(launch_basis(c->rec_p.p, c->W, c->K, c->N, c->bprog, c->V.p, c->Wpad,
                           c->series.p + 8 * size_t(s), nullptr, c->stream));
+    LEMC_TRY(multipole_step(c));
     if (hook) {
       if (!c->hooked) ++c->version;
       c->hooked = true;
@@ -1055,7 +1158,22 @@ int lemc_read_gram(lemc_ctx* c, int s, double* S, double* H2, double* H4, double
                                 cudaMemcpyDeviceToHost, c->stream));
   LEMC_TRY(lemc_synchronize(c));
   if (n_samples) *n_samples = double(c->meas) * c->W;
-  return LEMC_OK;
+  // undo the range factors; a non-finite sum (an FP32 overflow of the basis
+  // values or of the accumulation) is reported, never returned silently
+  const double* sc = c->row_scale.data() + c->basis.sector_first[s];
+  bool finite = true;
+  for (int h = 0; h < 3; ++h) {
+    if (!outs[h]) continue;
+    for (int a = 0; a < dim; ++a)
+      for (int b = 0; b < dim; ++b) {
+        const double f = 1.0 / (sc[a] * sc[b]);
+        double* e = outs[h] + 2 * (size_t(a) * dim + b);
+        e[0] *= f;
+        e[1] *= f;
+        finite = finite && std::isfinite(e[0]) && std::isfinite(e[1]);
+      }
+  }
+  return finite ? LEMC_OK : LEMC_ERR_NUMERIC;
 }
 
 int lemc_read_cross(lemc_ctx* c, int sa, int sb, double* Cuser, double* Ccos, double* Csin) {
@@ -1063,13 +1181,29 @@ int lemc_read_cross(lemc_ctx* c, int sa, int sb, double* Cuser, double* Ccos, do
   if (!c->has_basis) return LEMC_ERR_STATE;
   for (size_t q = 0; q < c->cross_pairs.size(); ++q) {
     if (c->cross_pairs[q].first != sa || c->cross_pairs[q].second != sb) continue;
-    const size_t n = size_t(c->basis.sector_dim[sa]) * c->basis.sector_dim[sb];
+    const int da = c->basis.sector_dim[sa], db = c->basis.sector_dim[sb];
+    const size_t n = size_t(da) * db;
     double* outs[3] = {Cuser, Ccos, Csin};
     for (int h = 0; h < 3; ++h)
       if (outs[h])
         LEMC_CUDA(cudaMemcpyAsync(outs[h], c->cross.p + 2 * c->cross_plane * h + 2 * c->cross_off[q],
                                   sizeof(double) * 2 * n, cudaMemcpyDeviceToHost, c->stream));
-    return lemc_synchronize(c);
+    LEMC_TRY(lemc_synchronize(c));
+    const double* ca = c->row_scale.data() + c->basis.sector_first[sa];
+    const double* cb = c->row_scale.data() + c->basis.sector_first[sb];
+    bool finite = true;
+    for (int h = 0; h < 3; ++h) {
+      if (!outs[h]) continue;
+      for (int a = 0; a < da; ++a)
+        for (int b = 0; b < db; ++b) {
+          const double f = 1.0 / (ca[a] * cb[b]);
+          double* e = outs[h] + 2 * (size_t(a) * db + b);
+          e[0] *= f;
+          e[1] *= f;
+          finite = finite && std::isfinite(e[0]) && std::isfinite(e[1]);
+        }
+    }
+    return finite ? LEMC_OK : LEMC_ERR_NUMERIC;
   }
   return LEMC_ERR_ARG;
 }
@@ -1276,6 +1410,57 @@ int lemc_tune_step(lemc_ctx* c, double target, double tol, int moves, float* sig
     }
   }
   return LEMC_ERR_NUMERIC;
+}
+
+int lemc_close_bin(lemc_ctx* c) {
+  if (!c) return LEMC_ERR_ARG;
+  if (!c->has_basis || c->cfg.guide != LEMC_GUIDE_LAUGHLIN) return LEMC_ERR_STATE;
+  if (c->meas == c->bin_last_meas) return LEMC_ERR_STATE;  // empty bin
+  LEMC_TRY(flush_tc(c));
+  std::vector<double> cur(6 * c->gram_plane);
+  LEMC_CUDA(cudaMemcpyAsync(cur.data(), c->gram.p, sizeof(double) * cur.size(),
+                            cudaMemcpyDeviceToHost, c->stream));
+  LEMC_TRY(lemc_synchronize(c));
+  std::vector<double> bin(cur);
+  if (!c->bin_last.empty())
+    for (size_t i = 0; i < bin.size(); ++i) bin[i] -= c->bin_last[i];
+  c->bins.push_back(std::move(bin));
+  c->bin_samples.push_back(double(c->meas - c->bin_last_meas) * c->W);
+  c->bin_last = std::move(cur);
+  c->bin_last_meas = c->meas;
+  return LEMC_OK;
+}
+
+int lemc_n_bins(const lemc_ctx* c, int* n) {
+  if (!c || !n) return LEMC_ERR_ARG;
+  *n = int(c->bins.size());
+  return LEMC_OK;
+}
+
+int lemc_read_gram_bin(lemc_ctx* c, int bin, int s, double* S, double* H2, double* H4,
+                       double* n_samples) {
+  if (!c) return LEMC_ERR_ARG;
+  if (bin < 0 || bin >= int(c->bins.size()) || s < 0 || s >= int(c->sec_row.size()))
+    return LEMC_ERR_ARG;
+  const int dim = c->basis.sector_dim[s];
+  const size_t off = 2 * size_t(c->sec_goff[s]);
+  const double* sc = c->row_scale.data() + c->basis.sector_first[s];
+  double* outs[3] = {S, H2, H4};
+  bool finite = true;
+  for (int h = 0; h < 3; ++h) {
+    if (!outs[h]) continue;
+    const double* src = c->bins[bin].data() + 2 * c->gram_plane * h + off;
+    for (int a = 0; a < dim; ++a)
+      for (int b = 0; b < dim; ++b) {
+        const double f = 1.0 / (sc[a] * sc[b]);
+        const size_t o = 2 * (size_t(a) * dim + b);
+        outs[h][o] = src[o] * f;
+        outs[h][o + 1] = src[o + 1] * f;
+        finite = finite && std::isfinite(outs[h][o]) && std::isfinite(outs[h][o + 1]);
+      }
+  }
+  if (n_samples) *n_samples = c->bin_samples[bin];
+  return finite ? LEMC_OK : LEMC_ERR_NUMERIC;
 }
 
 int lemc_tau_sokal(const double* x, int T, double c, double* tau) {

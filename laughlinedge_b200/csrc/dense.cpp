@@ -318,6 +318,117 @@ extern "C" int lemc_geneig(int D, const double* H, const double* M, double eps, 
   return status;
 }
 
+// Edge dynamic structure factor of one (dL = 0) + (dL) problem, reference
+// generalized_eigenproblem.cpp:54-95: drop row/column 0 (the Laughlin state),
+// solve h c = E m c with c^H m c = 1, and weight mode j by |(Vc - i Vs)[0, 1:] c_j|^2.
+extern "C" int lemc_dsf_weights(int D, const double* H, const double* M, const double* Vc,
+                                const double* Vs, double eps, double* energies, double* weights,
+                                int* n_modes) {
+  if (D < 2 || !H || !M || !Vc || !Vs || !energies || !weights) return LEMC_ERR_ARG;
+  const int n = D - 1;
+  std::vector<double> h(2 * size_t(n) * n), m(2 * size_t(n) * n), ev(n), vec(2 * size_t(n) * n);
+  for (int a = 0; a < n; ++a)
+    for (int b = 0; b < n; ++b) {
+      const size_t o = 2 * (size_t(a) * n + b), q = 2 * (size_t(a + 1) * D + (b + 1));
+      h[o] = H[q];
+      h[o + 1] = H[q + 1];
+      m[o] = M[q];
+      m[o + 1] = M[q + 1];
+    }
+  int rank = 0;
+  const int st = lemc_geneig(n, h.data(), m.data(), eps, ev.data(), vec.data(), &rank);
+  if (st != LEMC_OK) return st;
+  for (int j = 0; j < n; ++j) {
+    double re = 0, im = 0;
+    for (int a = 0; a < n; ++a) {
+      // v = Vc[0][a+1] - i Vs[0][a+1]
+      const double vr = Vc[2 * (a + 1)] + Vs[2 * (a + 1) + 1];
+      const double vi = Vc[2 * (a + 1) + 1] - Vs[2 * (a + 1)];
+      const double cr = vec[2 * (size_t(a) * n + j)], ci = vec[2 * (size_t(a) * n + j) + 1];
+      re += vr * cr - vi * ci;
+      im += vr * ci + vi * cr;
+    }
+    energies[j] = ev[j];
+    weights[j] = j < rank ? re * re + im * im : NAN;
+  }
+  if (n_modes) *n_modes = rank;
+  return LEMC_OK;
+}
+
+// Jackknife over bins of raw Gram sums (leave one bin out): the normalised
+// M, H (lemc_normalise) and the generalized eigenvalues (lemc_geneig) of the
+// full sums, with their jackknife standard errors
+// err^2 = (B-1)/B sum_b |x_(-b) - mean_(-b)|^2.
+extern "C" int lemc_jackknife_spectrum(int D, int n_bins, const double* S, const double* H2,
+                                       const double* H4, double omega, double kappa, double eps,
+                                       double* evals, double* evals_err, double* M_err,
+                                       double* H_err) {
+  if (D <= 0 || n_bins < 2 || !S || !H2 || !H4 || !evals || !evals_err) return LEMC_ERR_ARG;
+  const size_t P = 2 * size_t(D) * D;
+  std::vector<double> tot[3];
+  const double* in[3] = {S, H2, H4};
+  for (int h = 0; h < 3; ++h) {
+    tot[h].assign(P, 0.0);
+    for (int b = 0; b < n_bins; ++b)
+      for (size_t i = 0; i < P; ++i) tot[h][i] += in[h][size_t(b) * P + i];
+  }
+  std::vector<double> M(P), H(P);
+  int rank = 0;
+  int st = lemc_normalise(D, tot[0].data(), tot[1].data(), tot[2].data(), omega, kappa, M.data(),
+                          H.data());
+  if (st != LEMC_OK) return st;
+  st = lemc_geneig(D, H.data(), M.data(), eps, evals, nullptr, &rank);
+  if (st != LEMC_OK) return st;
+  std::vector<double> ev_b(size_t(n_bins) * D), M_b(size_t(n_bins) * P), H_b(size_t(n_bins) * P);
+  std::vector<double> part[3];
+  for (int h = 0; h < 3; ++h) part[h].resize(P);
+  for (int b = 0; b < n_bins; ++b) {
+    for (int h = 0; h < 3; ++h)
+      for (size_t i = 0; i < P; ++i) part[h][i] = tot[h][i] - in[h][size_t(b) * P + i];
+    st = lemc_normalise(D, part[0].data(), part[1].data(), part[2].data(), omega, kappa,
+                        M_b.data() + size_t(b) * P, H_b.data() + size_t(b) * P);
+    if (st != LEMC_OK) return st;
+    int rk = 0;
+    st = lemc_geneig(D, H_b.data() + size_t(b) * P, M_b.data() + size_t(b) * P, eps,
+                     ev_b.data() + size_t(b) * D, nullptr, &rk);
+    if (st != LEMC_OK) return st;
+  }
+  const double f = double(n_bins - 1) / n_bins;
+  for (int j = 0; j < D; ++j) {
+    double mean = 0;
+    for (int b = 0; b < n_bins; ++b) mean += ev_b[size_t(b) * D + j];
+    mean /= n_bins;
+    double var = 0;
+    for (int b = 0; b < n_bins; ++b) {
+      const double d = ev_b[size_t(b) * D + j] - mean;
+      var += d * d;
+    }
+    evals_err[j] = std::sqrt(f * var);
+  }
+  double* errs[2] = {M_err, H_err};
+  const std::vector<double>* samples[2] = {&M_b, &H_b};
+  for (int q = 0; q < 2; ++q) {
+    if (!errs[q]) continue;
+    for (size_t e = 0; e < P / 2; ++e) {
+      double mr = 0, mi = 0;
+      for (int b = 0; b < n_bins; ++b) {
+        mr += (*samples[q])[size_t(b) * P + 2 * e];
+        mi += (*samples[q])[size_t(b) * P + 2 * e + 1];
+      }
+      mr /= n_bins;
+      mi /= n_bins;
+      double var = 0;
+      for (int b = 0; b < n_bins; ++b) {
+        const double dr = (*samples[q])[size_t(b) * P + 2 * e] - mr;
+        const double di = (*samples[q])[size_t(b) * P + 2 * e + 1] - mi;
+        var += dr * dr + di * di;
+      }
+      errs[q][e] = std::sqrt(f * var);
+    }
+  }
+  return LEMC_OK;
+}
+
 extern "C" int lemc_normalise(int D, const double* S, const double* H2, const double* H4,
                               double omega, double kappa, double* Mout, double* Hout) {
   if (D <= 0 || !S) return LEMC_ERR_ARG;

@@ -434,3 +434,70 @@ extern "C" int lemc_evolve_device(int D, const double* M, const double* H, const
     return LEMC_ERR_CUDA;
   return LEMC_OK;
 }
+
+// Edge density on an angular grid from its Fourier components (reference
+// observer::edgeDensity_reconstruct, dynamics.cpp:110-125, gives the
+// components <rho_l>(t) = C^H rho_l C; the density itself is
+// n(theta) = (1/2pi) [<rho_0> + 2 Re sum_{l>0} e^{-i l theta} <rho_l>]).
+namespace lemc {
+namespace {
+
+__global__ void density_grid_kernel(int L, const int* __restrict__ ls, int n_times,
+                                    const double2* __restrict__ rho, const double2* __restrict__ ref,
+                                    int n_theta, double* __restrict__ out) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const int t = blockIdx.y;
+  if (g >= n_theta || t >= n_times) return;
+  const double theta = 2.0 * M_PI * double(g) / double(n_theta);
+  double acc = 0.0;
+  for (int q = 0; q < L; ++q) {
+    const double2 r = rho[size_t(t) * L + q];
+    const double2 r0 = ref[q];
+    const double dr = r.x - r0.x, di = r.y - r0.y;
+    const int l = ls[q];
+    if (l == 0) {
+      acc += dr;
+    } else {
+      double s, c;
+      sincos(double(l) * theta, &s, &c);
+      acc += 2.0 * (dr * c + di * s);  // 2 Re(e^{-i l theta} (dr + i di))
+    }
+  }
+  out[size_t(t) * n_theta + g] = acc / (2.0 * M_PI);
+}
+
+}  // namespace
+}  // namespace lemc
+
+extern "C" int lemc_edge_density_grid(int L, const int32_t* l, int n_times, const double* rho_t,
+                                      const double* rho_ref, int n_theta, double* out) {
+  using namespace lemc;
+  if (L <= 0 || !l || n_times <= 0 || !rho_t || n_theta <= 0 || !out) return LEMC_ERR_ARG;
+  for (int q = 0; q < L; ++q)
+    if (l[q] < 0) return LEMC_ERR_ARG;
+  int* d_l = nullptr;
+  double2 *d_rho = nullptr, *d_ref = nullptr;
+  double* d_out = nullptr;
+  int st = LEMC_OK;
+  auto ok = [&](cudaError_t e) {
+    if (e != cudaSuccess && st == LEMC_OK) st = LEMC_ERR_CUDA;
+    return st == LEMC_OK;
+  };
+  const size_t nr = size_t(n_times) * L;
+  if (ok(cudaMalloc(&d_l, sizeof(int) * L)) && ok(cudaMalloc(&d_rho, sizeof(double2) * nr)) &&
+      ok(cudaMalloc(&d_ref, sizeof(double2) * L)) &&
+      ok(cudaMalloc(&d_out, sizeof(double) * size_t(n_times) * n_theta)) &&
+      ok(cudaMemcpy(d_l, l, sizeof(int) * L, cudaMemcpyHostToDevice)) &&
+      ok(cudaMemcpy(d_rho, rho_t, sizeof(double2) * nr, cudaMemcpyHostToDevice)) &&
+      ok(cudaMemcpy(d_ref, rho_ref ? rho_ref : rho_t, sizeof(double2) * L, cudaMemcpyHostToDevice))) {
+    const dim3 grid((n_theta + 127) / 128, n_times);
+    density_grid_kernel<<<grid, 128>>>(L, d_l, n_times, d_rho, d_ref, n_theta, d_out);
+    if (ok(cudaGetLastError()))
+      ok(cudaMemcpy(out, d_out, sizeof(double) * size_t(n_times) * n_theta, cudaMemcpyDeviceToHost));
+  }
+  cudaFree(d_l);
+  cudaFree(d_rho);
+  cudaFree(d_ref);
+  cudaFree(d_out);
+  return st;
+}

@@ -54,6 +54,9 @@ struct BasisProgram {
   int n_seg = 0;
   int max_seg = 0;  // longest segment, in nodes
   const int* seg_dev = nullptr;  // n_seg + 1 segment starts (node indices), on the device
+  // per-V-row factor applied when a value is stored (the Re and Im rows of a
+  // state carry the same factor); nullptr stores the plain products
+  const float* row_scale = nullptr;
 };
 
 // One tile of the SIMT FP64 Gram accumulation: three weighted sums
@@ -86,6 +89,9 @@ int launch_init_walkers(float2* pos, int W, int N, float radius, uint32_t seed_l
 // series_idx (may be null): the walker-mean series goes to series + 8 * *series_idx
 int launch_basis(const float2* rec_p, int W, int K, int N, const BasisProgram& prog, float* V,
                  int ldv, double* series, const uint32_t* series_idx, cudaStream_t st);
+// plane[w] = scale * Re p_k[w] (the multipole potential's USER plane)
+int launch_multipole_plane(const float2* rec_p, int W, int K, int k, double scale, float* plane,
+                           cudaStream_t st);
 // Learned-proposal sweep (one walker per warp) with BF16 network weights wts;
 // same arguments, records and error conventions as launch_sweep (Laughlin guide).
 int launch_learned_sweep(const SweepArgs& a, const void* wts, cudaStream_t st);

@@ -74,6 +74,88 @@ def geneig_sweep(S, H2, H4, omegas, kappas, eps: float = 1e-12):
     return ev.reshape(len(om), D), rank.value
 
 
+def jackknife_spectrum(S_bins, H2_bins, H4_bins, omega, kappa, eps: float = 1e-12):
+    """Leave-one-bin-out jackknife of one sector's spectrum from per-bin raw Gram
+    sums ([B, D, D] complex each): (evals, evals_err, M_err, H_err)."""
+    lib = _lib.load()
+    B, D = S_bins.shape[0], S_bins.shape[1]
+    a = [np.ascontiguousarray(X, dtype=np.complex128).view(np.float64).ravel()
+         for X in (S_bins, H2_bins, H4_bins)]
+    ev, er = np.zeros(D), np.zeros(D)
+    me, he = np.zeros(D * D), np.zeros(D * D)
+    check(lib.lemc_jackknife_spectrum(D, B, dptr(a[0]), dptr(a[1]), dptr(a[2]), omega, kappa, eps,
+                                      dptr(ev), dptr(er), dptr(me), dptr(he)),
+          "lemc_jackknife_spectrum")
+    return ev, er, me.reshape(D, D), he.reshape(D, D)
+
+
+def dsf_weights(H, M, Vc, Vs, eps: float = 1e-12):
+    """Edge dynamic structure factor (energies, weights) of the normalised
+    {0, dL} matrices (row 0 = Laughlin state), liblemc's lemc_dsf_weights."""
+    lib = _lib.load()
+    D = H.shape[0]
+    a = [np.ascontiguousarray(X, dtype=np.complex128).view(np.float64).ravel() for X in (H, M, Vc, Vs)]
+    e, w = np.zeros(D - 1), np.zeros(D - 1)
+    n = C.c_int()
+    check(lib.lemc_dsf_weights(D, dptr(a[0]), dptr(a[1]), dptr(a[2]), dptr(a[3]), eps, dptr(e),
+                               dptr(w), C.byref(n)), "lemc_dsf_weights")
+    return e[: n.value], w[: n.value]
+
+
+def _herm(X):
+    return 0.5 * (X + X.conj().T)
+
+
+def dsf_compute(particles, inverse_filling, dL, n_walkers, burn_in, sweeps, omega, kappa,
+                step_sigma=0.3, seed=42, guide=_lib.GUIDE_LAUGHLIN, gram_mode=_lib.GRAM_FP64):
+    """Edge DSF of sector dL, as edgeMC::dsf_compute (em_dsf.cu:233-260): one
+    context over the sectors {0, dL} with the angular probe dL; normalised H, M
+    and the cos / sin(dL theta) excitation matrices, Hermitised, then
+    dsf_weights.  Returns (energies, weights, H, M, Vc, Vs)."""
+    smp = Sampler(SamplerConfig(particles, inverse_filling, n_walkers, step_sigma=step_sigma, seed=seed,
+                                guide=guide, gram_mode=gram_mode), [0, dL], probes=[dL])
+    try:
+        smp.init_walkers()
+        smp.run(burn_in, measure=False)
+        smp.run(sweeps, measure=True)
+        D = smp.total_dim
+        d0 = smp.dims[0]
+        M = np.zeros((D, D), complex)
+        H = np.zeros((D, D), complex)
+        Vc = np.zeros((D, D), complex)
+        Vs = np.zeros((D, D), complex)
+        if guide == _lib.GUIDE_ROW:
+            fg, gg, fh, n, fc, fs, _ = smp.rows(omega, kappa, extra=True)
+            sq = np.sqrt(gg)
+            sec = np.array([0] * d0 + [1] * (D - d0))
+            same = sec[:, None] == sec[None, :]
+            M[same], H[same] = (fg / sq)[same], (fh / sq)[same]
+            Vc[~same], Vs[~same] = (fc / sq)[~same], (fs / sq)[~same]
+        else:
+            nrm = []
+            first = 0
+            for si, d in enumerate(smp.dims):
+                S, H2, H4, _ = smp.gram(si)
+                Mn, Hn = normalise(S, H2, H4, omega, kappa)
+                M[first:first + d, first:first + d] = Mn
+                H[first:first + d, first:first + d] = Hn
+                nrm.extend(np.sqrt(np.real(np.diag(S))))
+                first += d
+            nrm = np.array(nrm)
+            for sa, sb in ((0, 1), (1, 0)):
+                _, cc, cs = smp.cross(sa, sb)
+                fa, fb = (0, d0) if sa == 0 else (d0, 0)
+                da, db = smp.dims[sa], smp.dims[sb]
+                den = np.outer(nrm[fa:fa + da], nrm[fb:fb + db])
+                Vc[fa:fa + da, fb:fb + db] = cc / den
+                Vs[fa:fa + da, fb:fb + db] = cs / den
+        H, M, Vc, Vs = _herm(H), _herm(M), _herm(Vc), _herm(Vs)
+        e, w = dsf_weights(H, M, Vc, Vs)
+        return e, w, H, M, Vc, Vs
+    finally:
+        smp.close()
+
+
 def normalise(S, H2=None, H4=None, omega=0.0, kappa=0.0):
     """Reference normalisation M = S/sqrt(S_aa S_bb), H = (w H2 + k H4)/sqrt(..), Hermitised."""
     lib = _lib.load()
@@ -254,6 +336,30 @@ class Sampler:
                 return -1
         self._hook = _lib.STEP_HOOK(_cb)
         check(self.lib.lemc_run_hooked(self._h, int(n_sweeps), self._hook, None), "lemc_run_hooked")
+
+    def close_bin(self):
+        """End the current bin of measurements (jackknife error bars)."""
+        check(self.lib.lemc_close_bin(self._h), "lemc_close_bin")
+
+    def n_bins(self) -> int:
+        n = C.c_int()
+        check(self.lib.lemc_n_bins(self._h, C.byref(n)), "lemc_n_bins")
+        return n.value
+
+    def gram_bin(self, bin_index: int, sector_index: int):
+        D = self.dims[sector_index]
+        bufs = [np.zeros(2 * D * D) for _ in range(3)]
+        n = C.c_double()
+        check(self.lib.lemc_read_gram_bin(self._h, bin_index, sector_index,
+                                          *[dptr(b) for b in bufs], C.byref(n)), "lemc_read_gram_bin")
+        return tuple(_cplx(b, D) for b in bufs) + (n.value,)
+
+    def jackknife(self, sector_index: int, omega: float, kappa: float, eps: float = 1e-12):
+        """Spectrum of one sector with jackknife errors over the closed bins:
+        (evals, evals_err, M_err, H_err)."""
+        bins = [self.gram_bin(b, sector_index) for b in range(self.n_bins())]
+        S, H2, H4 = (np.array([b[i] for b in bins]) for i in range(3))
+        return jackknife_spectrum(S, H2, H4, omega, kappa, eps)
 
     def set_step(self, sigma: float):
         check(self.lib.lemc_set_step(self._h, float(sigma)), "lemc_set_step")
