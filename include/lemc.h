@@ -406,6 +406,24 @@ LEMC_API int lemc_occupation(const lemc_occupation_config* cfg, double* out, dou
 LEMC_API int lemc_occupation_static(const lemc_occupation_config* cfg, double* out,
                                     double* acceptance);
 
+/* Edge spectral function of sector dL as energy-resolved orbital occupations:
+ * the occupation matrices occ (lemc_occupation's per-pair averages, D x D x
+ * Lc complex) normalised with the metric as the reference normalises them
+ * (gf_occupation_numbers.cu:432-445) and Hermitised per l, rotated onto the
+ * generalized eigenvectors c_j of H c = E M c (normalised H, M of the same
+ * sector, c^H M c = 1):
+ *   weights[j][l] = Re c_j^H n_l c_j,  sum_l weights[j][l] = N,
+ * with energies[j] ascending (*n_modes = kept rank; later rows NaN).
+ * A(l, E) = sum_j weights[j][l] delta(E - E_j) is the spectral weight of
+ * angular-momentum orbital l at edge energy E.  The reference announces a
+ * spectral function on its two-state walker but leaves it unimplemented
+ * (README.md:14-15; the commented spectral_function_sampler,
+ * green_function.h:90); this is the rotation onto the eigenvector basis that
+ * its occupation output asks for (gf_occupation_numbers.cu:512).  Host only. */
+LEMC_API int lemc_spectral_weights(int D, int Lc, const double* occ, const double* H,
+                                   const double* M, int N, double eps, double* energies,
+                                   double* weights, int* n_modes);
+
 /* ---- FP64 dense tail ----------------------------------------------------
  * Generalized Hermitian eigenproblem H c = E M c (complex D x D, interleaved).
  * Eigenvalues ascending; eigenvectors (optional, column j = vector j) are

@@ -8,10 +8,11 @@ from ._lib import LemcError, load
 from .dynamics import density_grid, edge_response
 from .proposal import LearnedProposal
 from .sampler import (Sampler, SamplerConfig, dsf_compute, dsf_weights, evolve, evolve_device, geneig,
-                      geneig_sweep, jackknife_spectrum, normalise, partitions, series_tau, tau_binning,
-                      tau_sokal)
+                      geneig_sweep, jackknife_spectrum, normalise, occupation, partitions, series_tau,
+                      spectral_function, spectral_weights, tau_binning, tau_sokal)
 
 __all__ = ["LearnedProposal", "LemcError", "Sampler", "SamplerConfig", "density_grid", "dsf_compute",
            "dsf_weights", "edge_response", "evolve",
-           "evolve_device", "geneig", "geneig_sweep", "jackknife_spectrum", "load", "normalise", "partitions", "series_tau",
+           "evolve_device", "geneig", "geneig_sweep", "jackknife_spectrum", "load", "occupation",
+           "spectral_function", "spectral_weights", "normalise", "partitions", "series_tau",
            "tau_binning", "tau_sokal", "_lib"]

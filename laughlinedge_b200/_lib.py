@@ -117,6 +117,7 @@ _SIGNATURES = {
     "lemc_basis_device": ([_P, _P, _I, _P, _I, _P], _I),
     "lemc_gram_device": ([_P, _P, _P, _I, _I, _I, _P], _I),
     "lemc_geneig": ([_I, _DP, _DP, _D, _DP, _DP, _IP], _I),
+    "lemc_spectral_weights": ([_I, _I, _DP, _DP, _DP, _I, _D, _DP, _DP, _IP], _I),
     "lemc_dsf_weights": ([_I, _DP, _DP, _DP, _DP, _D, _DP, _DP, _IP], _I),
     "lemc_proposal_n_params": ([_IP], _I),
     "lemc_proposal_create": ([_I, _I, C.c_float, C.c_uint64, C.POINTER(_P)], _I),

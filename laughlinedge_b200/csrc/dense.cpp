@@ -429,6 +429,65 @@ extern "C" int lemc_jackknife_spectrum(int D, int n_bins, const double* S, const
   return LEMC_OK;
 }
 
+// Energy-resolved edge occupations: the occupation matrices of one sector,
+// normalised as the reference does with the metric (gf_occupation_numbers.cu:
+// 432-445: n_l(L,R) = occ_l(L,R) / sum_l occ_l(L,R) * N * M(L,R), then made
+// Hermitian per l), rotated onto the generalized eigenvectors of H c = E M c
+// (c^H M c = 1): w_j(l) = Re c_j^H n_l c_j, so that sum_l w_j(l) = N.
+extern "C" int lemc_spectral_weights(int D, int Lc, const double* occ, const double* H,
+                                     const double* M, int N, double eps, double* energies,
+                                     double* weights, int* n_modes) {
+  if (D <= 0 || Lc <= 0 || !occ || !H || !M || N <= 0 || !energies || !weights) return LEMC_ERR_ARG;
+  using cd = std::complex<double>;
+  std::vector<cd> n(size_t(D) * D * Lc);
+  for (int a = 0; a < D; ++a)
+    for (int b = 0; b < D; ++b) {
+      cd sum = 0;
+      for (int l = 0; l < Lc; ++l) {
+        const size_t o = 2 * ((size_t(a) * D + b) * Lc + l);
+        sum += cd(occ[o], occ[o + 1]);
+      }
+      if (std::abs(sum) == 0) return LEMC_ERR_NUMERIC;
+      const cd mab(M[2 * (size_t(a) * D + b)], M[2 * (size_t(a) * D + b) + 1]);
+      for (int l = 0; l < Lc; ++l) {
+        const size_t o = (size_t(a) * D + b) * Lc + l;
+        n[o] = cd(occ[2 * o], occ[2 * o + 1]) / sum * double(N) * mab;
+      }
+    }
+  for (int l = 0; l < Lc; ++l)
+    for (int a = 0; a < D; ++a)
+      for (int b = a; b < D; ++b) {
+        const size_t ab = (size_t(a) * D + b) * Lc + l, ba = (size_t(b) * D + a) * Lc + l;
+        const cd v = 0.5 * (n[ab] + std::conj(n[ba]));
+        n[ab] = v;
+        n[ba] = std::conj(v);
+      }
+  std::vector<double> vec(2 * size_t(D) * D);
+  int rank = 0;
+  const int st = lemc_geneig(D, H, M, eps, energies, vec.data(), &rank);
+  if (st != LEMC_OK) return st;
+  for (int j = 0; j < D; ++j)
+    for (int l = 0; l < Lc; ++l) {
+      if (j >= rank) {
+        weights[size_t(j) * Lc + l] = NAN;
+        continue;
+      }
+      cd acc = 0;
+      for (int a = 0; a < D; ++a) {
+        const cd ca(vec[2 * (size_t(a) * D + j)], vec[2 * (size_t(a) * D + j) + 1]);
+        cd row = 0;
+        for (int b = 0; b < D; ++b) {
+          const cd cb(vec[2 * (size_t(b) * D + j)], vec[2 * (size_t(b) * D + j) + 1]);
+          row += n[(size_t(a) * D + b) * Lc + l] * cb;
+        }
+        acc += std::conj(ca) * row;
+      }
+      weights[size_t(j) * Lc + l] = acc.real();
+    }
+  if (n_modes) *n_modes = rank;
+  return LEMC_OK;
+}
+
 extern "C" int lemc_normalise(int D, const double* S, const double* H2, const double* H4,
                               double omega, double kappa, double* Mout, double* Hout) {
   if (D <= 0 || !S) return LEMC_ERR_ARG;

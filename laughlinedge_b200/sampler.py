@@ -256,6 +256,42 @@ def series_tau(series: np.ndarray):
             "binning_plateau": bool(conv), "series_length": int(series.shape[0])}
 
 
+def spectral_weights(occ, H, M, particles, eps: float = 1e-12):
+    """Energy-resolved occupations of one sector (lemc_spectral_weights):
+    (energies [D], weights [D, Lc]) with sum_l weights[j, l] = particles."""
+    lib = _lib.load()
+    D, Lc = occ.shape[0], occ.shape[2]
+    o = np.ascontiguousarray(occ, dtype=np.complex128).view(np.float64).ravel()
+    h = np.ascontiguousarray(H, dtype=np.complex128).view(np.float64).ravel()
+    m = np.ascontiguousarray(M, dtype=np.complex128).view(np.float64).ravel()
+    e, w = np.zeros(D), np.zeros(D * Lc)
+    n = C.c_int()
+    check(lib.lemc_spectral_weights(D, Lc, dptr(o), dptr(h), dptr(m), particles, eps, dptr(e),
+                                    dptr(w), C.byref(n)), "lemc_spectral_weights")
+    return e, w.reshape(D, Lc)
+
+
+def spectral_function(particles, inverse_filling, dL, omega, kappa, n_walkers=8192, burn_in=500,
+                      sweeps=2000, l_cutoff=None, step_sigma=0.3, seed=42):
+    """Edge spectral function of sector dL: the normalised M, H of the sector
+    (shared-guide sampler) and its occupation matrices (two-state walker),
+    combined by spectral_weights.  Returns (energies, weights [D, l_cutoff])."""
+    Lc = l_cutoff or inverse_filling * (particles - 1) + 15
+    smp = Sampler(SamplerConfig(particles, inverse_filling, n_walkers, step_sigma=step_sigma, seed=seed),
+                  [dL])
+    try:
+        smp.init_walkers()
+        smp.run(burn_in, measure=False)
+        smp.run(sweeps, measure=True)
+        S, H2, H4, _ = smp.gram(0)
+    finally:
+        smp.close()
+    M, H = normalise(S, H2, H4, omega, kappa)
+    occ, _ = occupation(particles, inverse_filling, dL, Lc, n_walkers, sweeps, burn_in=burn_in,
+                        step_sigma=step_sigma, seed=seed + 1)
+    return spectral_weights(occ, H, M, particles)
+
+
 @dataclass
 class SamplerConfig:
     particles: int
