@@ -75,7 +75,9 @@ typedef struct lemc_config {
   int32_t inverse_filling;  /* m (nu = 1/m)                                   */
   int32_t n_walkers;        /* W, independent Markov chains                  */
   int32_t lanes_per_walker; /* G in {1,2,4,8,16,32}; 0 = heuristic, -1 = autotuned at
-                               lemc_init_walkers by timing every feasible G    */
+                               lemc_init_walkers by timing every feasible G, and
+                               (tensor-core modes) the contraction's walker split
+                               at the first measured sweep                      */
   float step_sigma;         /* Gaussian single-particle step (l_B)           */
   int32_t guide;            /* enum lemc_guide                               */
   uint64_t seed;            /* Philox-4x32-10 key                            */
@@ -149,6 +151,9 @@ LEMC_API int lemc_tune_step(lemc_ctx* ctx, double target, double tol, int moves,
                             double* acceptance);
 /* Walker width G in use (after autotuning). */
 LEMC_API int lemc_lanes_per_walker(const lemc_ctx* ctx, int* lanes);
+/* Walker split of the tensor-core contraction (jobs = tiles x split; 0 before
+ * the first contraction without autotuning). */
+LEMC_API int lemc_gram_splits(const lemc_ctx* ctx, int* splits);
 /* Select the angular-momentum sectors whose basis is sampled. */
 LEMC_API int lemc_set_sectors(lemc_ctx* ctx, const int32_t* sectors, int n_sectors);
 /* Guide rows for LEMC_GUIDE_ROW: walker w samples |P_{rows[w % n]}|^2 |Psi|^2,
@@ -188,8 +193,19 @@ LEMC_API int lemc_run(lemc_ctx* ctx, int n_sweeps, int measure);
 typedef int (*lemc_step_hook)(void* user, const float* dev_xy, float* dev_user_plane, int W,
                               int N, void* stream);
 LEMC_API int lemc_run_hooked(lemc_ctx* ctx, int n_sweeps, lemc_step_hook hook, void* user);
-/* Zero every accumulator (samples, Gram matrices, series, acceptance). */
+/* Zero every accumulator (samples, Gram matrices, series, acceptance) and the
+ * context's device error word (after LEMC_ERR_TIMEOUT the context is usable
+ * again once reset). */
 LEMC_API int lemc_reset_accumulators(lemc_ctx* ctx);
+/* Bounded waits of the tensor-core contraction.  Every mbarrier wait of
+ * gram_tc_kernel gives up after `cycles` SM clocks (0 restores the default,
+ * about 2 s); the kernel then records LEMC_ERR_TIMEOUT in the context's error
+ * word, waits (bounded) for its own copies and MMAs in flight, frees its
+ * tensor memory and exits, and lemc_synchronize / the read calls return
+ * LEMC_ERR_TIMEOUT.  hold_loads != 0 keeps the kernel's loader from issuing
+ * any copy, so that every wait expires: a test hook for that path (process
+ * wide, for launches made afterwards).  No counterpart in the reference. */
+LEMC_API int lemc_debug_gram_wait(long long cycles, int hold_loads);
 LEMC_API int lemc_synchronize(lemc_ctx* ctx);
 /* The context's CUDA stream (cudaStream_t), for callers that order their own
  * work or device timers after the context's kernels. */

@@ -86,6 +86,7 @@ _SIGNATURES = {
     "lemc_destroy": ([_P], _I),
     "lemc_set_sectors": ([_P, _I32P, _I], _I),
     "lemc_lanes_per_walker": ([_P, _IP], _I),
+    "lemc_gram_splits": ([_P, _IP], _I),
     "lemc_set_guide_rows": ([_P, _I32P, _I], _I),
     "lemc_init_walkers": ([_P, _FP], _I),
     "lemc_run": ([_P, _I, _I], _I),
@@ -105,6 +106,7 @@ _SIGNATURES = {
     "lemc_read_positions": ([_P, _FP], _I),
     "lemc_read_series": ([_P, _DP, _I, _IP], _I),
     "lemc_tau_sokal": ([_DP, _I, _D, _DP], _I),
+    "lemc_debug_gram_wait": ([C.c_longlong, _I], _I),
     "lemc_close_bin": ([_P], _I),
     "lemc_n_bins": ([_P, _IP], _I),
     "lemc_read_gram_bin": ([_P, _I, _I, _DP, _DP, _DP, _DP], _I),

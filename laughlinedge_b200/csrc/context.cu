@@ -180,6 +180,8 @@ struct lemc_ctx {
   std::vector<double> row_scale;      // per basis row
   DevBuf<float> d_row_scale;          // per V row
   bool scale_pending = false;
+  bool gram_tune_pending = false;  // autotune the contraction's walker split
+  int gram_splits = 0;             // the tuned split (0: one-wave rule)
 
   std::vector<int> probes;  // angular probes l_q
   // guide rows
@@ -345,7 +347,7 @@ int alloc_records(lemc_ctx* c) {
   return LEMC_OK;
 }
 
-int setup_tc(lemc_ctx* c);
+int setup_tc(lemc_ctx* c, int force_splits = 0);
 
 // SIMT job list: same-sector Gram tiles {ONE, R2, R4} and, for every ordered
 // pair of sectors (diagonal pairs included), cross tiles {USER, COS_l, SIN_l}
@@ -489,7 +491,7 @@ int gram_step(lemc_ctx* c, const float* V, const float* rec_w, int ldw, int W, i
                             c->n_gram_jobs + (cross ? c->n_cross_jobs : 0), splits, c->gram.p,
                             c->gram_plane, c->cross.p, c->cross_plane, c->stream);
   }
-  if (c->tc_tiles.empty()) LEMC_TRY(setup_tc(c));
+  if (c->tc_tiles.empty()) LEMC_TRY(setup_tc(c, c->gram_splits));
   int s = launch_gram_tc_rows(V, c->Wpad, 2 * c->D, rec_w, ldw, c->Wpad, c->d_tc_tiles.p,
                               int(c->tc_tiles.size()), c->tc_splits, c->tc_partials.p, mode,
                               c->cfg.flush_every, c->err.p, c->stream);
@@ -503,7 +505,7 @@ int gram_step(lemc_ctx* c, const float* V, const float* rec_w, int ldw, int W, i
   return s;
 }
 
-int setup_tc(lemc_ctx* c) {
+int setup_tc(lemc_ctx* c, int force_splits) {
   // Sector-aligned panels: consecutive sectors of at most 128 V rows are packed
   // into one 128-row A panel with 32-row B panels over the group's rows; a
   // larger sector gets its own 128-row A slices x 32-row B panels.
@@ -545,8 +547,9 @@ int setup_tc(lemc_ctx* c) {
   c->tc_ntiles = nt;
   c->tc_maxdim = 0;
   for (int d : c->basis.sector_dim) c->tc_maxdim = std::max(c->tc_maxdim, d);
-  // one wave: at most one job per SM
-  c->tc_splits = std::max(1, std::min(sm / std::max(1, nt), c->Wpad / 128));
+  // one wave: at most one job per SM (unless the autotuner chose the split)
+  c->tc_splits = force_splits > 0 ? std::min(force_splits, std::max(1, c->Wpad / 128))
+                                  : std::max(1, std::min(sm / std::max(1, nt), c->Wpad / 128));
   c->tc_tiles.clear();
   for (int sp = 0; sp < c->tc_splits; ++sp)
     for (int t = 0; t < nt; ++t)
@@ -762,6 +765,9 @@ int lemc_set_sectors(lemc_ctx* c, const int32_t* sectors, int n) {
   }
   c->bprog.row_scale = c->d_row_scale.p;
   c->scale_pending = c->cfg.guide == LEMC_GUIDE_LAUGHLIN;
+  c->gram_tune_pending = c->cfg.lanes_per_walker < 0 && c->cfg.guide == LEMC_GUIDE_LAUGHLIN &&
+                         c->cfg.gram_mode != LEMC_GRAM_FP64;
+  c->gram_splits = 0;
   c->tc_tiles.clear();
   LEMC_TRY(upload_guide(c));
   return lemc_reset_accumulators(c);
@@ -827,6 +833,12 @@ static int autotune_lanes(lemc_ctx* c) {
   return LEMC_OK;
 }
 
+int lemc_gram_splits(const lemc_ctx* c, int* splits) {
+  if (!c || !splits) return LEMC_ERR_ARG;
+  *splits = c->tc_tiles.empty() ? c->gram_splits : c->tc_splits;
+  return LEMC_OK;
+}
+
 int lemc_lanes_per_walker(const lemc_ctx* c, int* G) {
   if (!c || !G) return LEMC_ERR_ARG;
   *G = c->G;
@@ -856,6 +868,7 @@ int lemc_reset_accumulators(lemc_ctx* c) {
   if (c->tc_partials.p)
     LEMC_CUDA(cudaMemsetAsync(c->tc_partials.p, 0, sizeof(double) * c->tc_partials.n, c->stream));
   if (c->accepted.p) LEMC_CUDA(cudaMemsetAsync(c->accepted.p, 0, 4 * c->W, c->stream));
+  if (c->err.p) LEMC_CUDA(cudaMemsetAsync(c->err.p, 0, sizeof(int), c->stream));
   c->meas = 0;
   c->bins.clear();
   c->bin_samples.clear();
@@ -972,7 +985,7 @@ static int ensure_graph(lemc_ctx* c, int G) {
   // everything the captured launches point at must exist before capture
   LEMC_TRY(c->d_ctr.alloc(2));
   if (c->cfg.guide != LEMC_GUIDE_ROW && c->cfg.gram_mode != LEMC_GRAM_FP64 && c->tc_tiles.empty())
-    LEMC_TRY(setup_tc(c));
+    LEMC_TRY(setup_tc(c, c->gram_splits));
   cudaGraph_t g = nullptr;
   LEMC_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed));
   int st = LEMC_OK;
@@ -1045,6 +1058,70 @@ static int compute_row_scales(lemc_ctx* c) {
   return LEMC_OK;
 }
 
+// Contraction autotuner (lanes_per_walker < 0, tensor-core modes): the walker
+// split of the tcgen05 jobs decides how many CTAs a launch has (tiles x split)
+// and how full its last wave is.  On a copy of the walkers, one sweep and one
+// basis build fill V; each candidate split (the one-wave rule, and the splits
+// that give 1, 2, 3 or 4 full waves of jobs) is timed over three launches
+// (best of two), the fastest kept.  The walkers are restored and the
+// accumulators zeroed, so the chain and its sums are those of an untuned run.
+static int autotune_gram_splits(lemc_ctx* c) {
+  int sm = 148, dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, dev);
+  LEMC_TRY(setup_tc(c, 0));
+  const int nt = c->tc_ntiles, smax = std::max(1, c->Wpad / 128);
+  std::vector<int> cand{c->tc_splits};
+  for (int waves = 1; waves <= 4; ++waves) {
+    const int sp = std::min(smax, std::max(1, (waves * sm) / std::max(1, nt)));
+    if (std::find(cand.begin(), cand.end(), sp) == cand.end()) cand.push_back(sp);
+  }
+  DevBuf<float2> save;
+  LEMC_TRY(save.alloc(size_t(c->W) * c->N));
+  LEMC_CUDA(cudaMemcpyAsync(save.p, c->pos.p, sizeof(float2) * c->W * c->N,
+                            cudaMemcpyDeviceToDevice, c->stream));
+  LEMC_TRY(sweep_once(c, 1, 1));
+  LEMC_TRY(launch_basis(c->rec_p.p, c->W, c->K, c->N, c->bprog, c->V.p, c->Wpad, nullptr,
+                        nullptr, c->stream));
+  float best = 1e30f;
+  int best_sp = cand[0];
+  for (int sp : cand) {
+    LEMC_TRY(setup_tc(c, sp));
+    auto launch = [&]() {
+      return launch_gram_tc_rows(c->V.p, c->Wpad, 2 * c->D, c->rec_w.p, c->Wpad, c->Wpad,
+                                 c->d_tc_tiles.p, int(c->tc_tiles.size()), c->tc_splits,
+                                 c->tc_partials.p, c->cfg.gram_mode, c->cfg.flush_every, c->err.p,
+                                 c->stream);
+    };
+    LEMC_TRY(launch());  // warm
+    float ms = 1e30f;
+    for (int rep = 0; rep < 2; ++rep) {
+      LEMC_CUDA(cudaEventRecord(c->ev[0], c->stream));
+      for (int k = 0; k < 3; ++k) LEMC_TRY(launch());
+      LEMC_CUDA(cudaEventRecord(c->ev[1], c->stream));
+      LEMC_CUDA(cudaEventSynchronize(c->ev[1]));
+      float t = 0;
+      cudaEventElapsedTime(&t, c->ev[0], c->ev[1]);
+      ms = std::min(ms, t);
+    }
+    if (ms < best) {
+      best = ms;
+      best_sp = sp;
+    }
+  }
+  c->gram_splits = best_sp;
+  LEMC_TRY(setup_tc(c, best_sp));
+  LEMC_CUDA(cudaMemcpyAsync(c->pos.p, save.p, sizeof(float2) * c->W * c->N,
+                            cudaMemcpyDeviceToDevice, c->stream));
+  if (c->accepted.p) LEMC_CUDA(cudaMemsetAsync(c->accepted.p, 0, 4 * c->W, c->stream));
+  LEMC_CUDA(cudaMemsetAsync(c->tc_partials.p, 0, sizeof(double) * c->tc_partials.n, c->stream));
+  LEMC_CUDA(cudaMemsetAsync(c->gram.p, 0, sizeof(double) * c->gram.n, c->stream));
+  LEMC_CUDA(cudaStreamSynchronize(c->stream));
+  ++c->version;
+  save.release();
+  return lemc_synchronize(c);
+}
+
 static int run_impl(lemc_ctx* c, int n_sweeps, int measure, lemc_step_hook hook, void* user) {
   if (!c || n_sweeps < 0) return LEMC_ERR_ARG;
   if (!c->walkers_ready) return LEMC_ERR_STATE;
@@ -1063,6 +1140,10 @@ static int run_impl(lemc_ctx* c, int n_sweeps, int measure, lemc_step_hook hook,
   if (c->scale_pending && c->meas == 0) {
     LEMC_TRY(compute_row_scales(c));
     c->scale_pending = false;
+  }
+  if (c->gram_tune_pending && c->meas == 0) {
+    LEMC_TRY(autotune_gram_splits(c));
+    c->gram_tune_pending = false;
   }
   LEMC_TRY(c->series.alloc(size_t(8) * n_sweeps));
   LEMC_CUDA(cudaMemsetAsync(c->series.p, 0, sizeof(double) * 8 * n_sweeps, c->stream));
@@ -1410,6 +1491,10 @@ int lemc_tune_step(lemc_ctx* c, double target, double tol, int moves, float* sig
     }
   }
   return LEMC_ERR_NUMERIC;
+}
+
+int lemc_debug_gram_wait(long long cycles, int hold_loads) {
+  return set_gram_wait(cycles, hold_loads);
 }
 
 int lemc_close_bin(lemc_ctx* c) {

@@ -44,7 +44,9 @@
 // stages at 384 and 448 (hi at +0, lo at +32).
 // No load uses cluster multicast; every source is this GPU's own memory.
 // Every mbarrier wait is bounded in time; on expiry the kernel records
-// LEMC_ERR_TIMEOUT in the error word, skips its output and unwinds.
+// LEMC_ERR_TIMEOUT in the error word, skips its output and unwinds: the loader
+// first waits (bounded) for the TMA copies it has in flight and the issuer for
+// the MMAs it has committed, then the CTA frees its tensor memory and exits.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -76,7 +78,7 @@ constexpr int kTmemCols = 512;
 constexpr uint32_t kColHH = 0;     // hi*hi buffers at 0 and 128
 constexpr uint32_t kColCorr = 256; // corrections
 constexpr uint32_t kColA = 384;    // A stages at 384 + 64 s (hi +0, lo +32)
-constexpr long long kWaitCycles = 4000000000LL;  // ~2 s at 1.9 GHz
+constexpr long long kWaitCycles = 4000000000LL;  // default wait bound, ~2 s at 1.9 GHz
 
 template <bool TF32>
 struct Cfg {
@@ -148,18 +150,34 @@ __device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
 }
 
 // Bounded wait; returns false (raising the CTA abort flag and the global error
-// word) when the phase does not complete in time or another role gave up.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* abort_flag, int* err) {
+// word) when the phase does not complete within `limit` cycles or another
+// role gave up.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* abort_flag, int* err,
+                                          long long limit) {
   const long long t0 = clock64();
   while (!mbar_try(bar, parity)) {
     if (*(volatile int*)abort_flag) return false;
-    if (clock64() - t0 > kWaitCycles) {
+    if (clock64() - t0 > limit) {
       *(volatile int*)abort_flag = 1;
       if (err) atomicExch(err, LEMC_ERR_TIMEOUT);
       return false;
     }
   }
   return true;
+}
+
+// Bounded wait for this CTA's own asynchronous work (its TMA copies, its
+// committed MMAs) that does not give up when another role aborted: those
+// operations complete by themselves, and the CTA must not release shared or
+// tensor memory while they are in flight.
+__device__ __forceinline__ void mbar_drain(uint64_t* bar, uint32_t parity, int* err, long long limit) {
+  const long long t0 = clock64();
+  while (!mbar_try(bar, parity)) {
+    if (clock64() - t0 > limit) {
+      if (err) atomicExch(err, LEMC_ERR_TIMEOUT);
+      return;
+    }
+  }
 }
 
 // Tiled 2D TMA load (no multicast) completing on an mbarrier transaction count.
@@ -304,6 +322,8 @@ struct TcArgs {
   int flush_every;
   int passes;           // 3 or 4
   int* err;
+  long long wait_cycles;  // bound of every mbarrier wait
+  int hold_loads;         // test hook: the loader issues nothing (the waits then expire)
 };
 
 template <bool TF32>
@@ -365,9 +385,10 @@ gram_tc_kernel(const TcArgs a, const __grid_constant__ CUtensorMap tmA,
     // ------------------------------- loader --------------------------------
     if (lane == 0) {
       const uint32_t tx_bytes = uint32_t(C::A_BYTES + C::B_BYTES + C::W_BYTES);
-      for (int c = 0; c < nch; ++c) {
+      int issued = 0;
+      for (int c = 0; c < nch && !a.hold_loads; ++c) {
         const int s = c % RS;
-        if (!mbar_wait(&sm->raw_empty[s], (uint32_t(c / RS) & 1u) ^ 1u, abort_flag, a.err)) break;
+        if (!mbar_wait(&sm->raw_empty[s], (uint32_t(c / RS) & 1u) ^ 1u, abort_flag, a.err, a.wait_cycles)) break;
         const int k0 = (c_beg + c) * KC;
         uint8_t* dst = sm->raw[s];
         mbar_arrive_tx(&sm->raw_full[s], tx_bytes);
@@ -376,7 +397,12 @@ gram_tc_kernel(const TcArgs a, const __grid_constant__ CUtensorMap tmA,
           tma_load_2d(dst + j * (kM * 128), &tmA, k0 + 32 * j, tile.row0, &sm->raw_full[s]);
         tma_load_2d(dst + C::A_BYTES, &tmB, k0, tile.col0, &sm->raw_full[s]);
         tma_load_2d(dst + C::A_BYTES + C::B_BYTES, &tmW, k0, 0, &sm->raw_full[s]);
+        ++issued;
       }
+      // the copies still in flight land before the CTA may exit, whatever the
+      // other roles did: the last one issued into each stage
+      for (int c = max(0, issued - RS); c < issued; ++c)
+        mbar_drain(&sm->raw_full[c % RS], uint32_t(c / RS) & 1u, a.err, a.wait_cycles);
     }
     __syncwarp();
   } else if (warp >= kAConvWarp0 && warp < kBConvWarp0) {
@@ -389,8 +415,8 @@ gram_tc_kernel(const TcArgs a, const __grid_constant__ CUtensorMap tmA,
     const uint32_t lane_base = uint32_t(quarter * 32) << 16;
     for (int c = 0; c < nch; ++c) {
       const int rs = c % RS, os = c % kOpStages;
-      if (!mbar_wait(&sm->raw_full[rs], uint32_t(c / RS) & 1u, abort_flag, a.err)) break;
-      if (!mbar_wait(&sm->op_empty[os], (uint32_t(c / kOpStages) & 1u) ^ 1u, abort_flag, a.err)) break;
+      if (!mbar_wait(&sm->raw_full[rs], uint32_t(c / RS) & 1u, abort_flag, a.err, a.wait_cycles)) break;
+      if (!mbar_wait(&sm->op_empty[os], (uint32_t(c / kOpStages) & 1u) ^ 1u, abort_flag, a.err, a.wait_cycles)) break;
       tc_fence_after();
       const uint8_t* raw = sm->raw[rs];
       const uint32_t a_hi = tmem + lane_base + kColA + uint32_t(os * 64);
@@ -438,8 +464,8 @@ gram_tc_kernel(const TcArgs a, const __grid_constant__ CUtensorMap tmA,
     const int t = threadIdx.x - kBConvWarp0 * 32;
     for (int c = 0; c < nch; ++c) {
       const int rs = c % RS, os = c % kOpStages;
-      if (!mbar_wait(&sm->raw_full[rs], uint32_t(c / RS) & 1u, abort_flag, a.err)) break;
-      if (!mbar_wait(&sm->op_empty[os], (uint32_t(c / kOpStages) & 1u) ^ 1u, abort_flag, a.err)) break;
+      if (!mbar_wait(&sm->raw_full[rs], uint32_t(c / RS) & 1u, abort_flag, a.err, a.wait_cycles)) break;
+      if (!mbar_wait(&sm->op_empty[os], (uint32_t(c / kOpStages) & 1u) ^ 1u, abort_flag, a.err, a.wait_cycles)) break;
       const uint8_t* rawb = sm->raw[rs] + C::A_BYTES;
       const float* rw = reinterpret_cast<const float*>(sm->raw[rs] + C::A_BYTES + C::B_BYTES);
       uint8_t* b_hi = sm->bop[os];
@@ -503,10 +529,10 @@ gram_tc_kernel(const TcArgs a, const __grid_constant__ CUtensorMap tmA,
       if (lane == 0 && !*(volatile int*)abort_flag) {
         bool ok = true;
         if (f == 0) {
-          ok = mbar_wait(&sm->acc_empty[b], ((ph_acc >> b) & 1u) ^ 1u, abort_flag, a.err);
+          ok = mbar_wait(&sm->acc_empty[b], ((ph_acc >> b) & 1u) ^ 1u, abort_flag, a.err, a.wait_cycles);
           ph_acc ^= 1u << b;
         }
-        if (ok) mbar_wait(&sm->op_full[s], ph_op, abort_flag, a.err);
+        if (ok) mbar_wait(&sm->op_full[s], ph_op, abort_flag, a.err, a.wait_cycles);
       }
       __syncwarp();
       named_arrive(1 + (c & 1));
@@ -571,7 +597,7 @@ gram_tc_kernel(const TcArgs a, const __grid_constant__ CUtensorMap tmA,
     if (lane == 0 && issued > 0) {
       // every issued MMA must retire before TMEM is released
       umma_commit(&sm->done);
-      mbar_wait(&sm->done, 0u, abort_flag, a.err);
+      mbar_drain(&sm->done, 0u, a.err, a.wait_cycles);
     }
     __syncwarp();
   } else if (warp < kEpiWarps) {
@@ -589,7 +615,7 @@ gram_tc_kernel(const TcArgs a, const __grid_constant__ CUtensorMap tmA,
     bool ok = true;
     for (int q = 0; q < nint; ++q) {
       const int b = q & 1;
-      if (!mbar_wait(&sm->acc_full[b], uint32_t(q >> 1) & 1u, abort_flag, a.err)) {
+      if (!mbar_wait(&sm->acc_full[b], uint32_t(q >> 1) & 1u, abort_flag, a.err, a.wait_cycles)) {
         ok = false;
         break;
       }
@@ -613,7 +639,7 @@ gram_tc_kernel(const TcArgs a, const __grid_constant__ CUtensorMap tmA,
         }
       }
     }
-    if (ok && nch > 0 && mbar_wait(&sm->corr_full, 0u, abort_flag, a.err)) {
+    if (ok && nch > 0 && mbar_wait(&sm->corr_full, 0u, abort_flag, a.err, a.wait_cycles)) {
       tc_fence_after();
       const uint32_t ta = tmem + lane_base + kColCorr + uint32_t(part0);
 #pragma unroll
@@ -746,7 +772,18 @@ int launch_t(const TcArgs& a, int n_jobs, cudaStream_t st) {
   return cudaPeekAtLastError() == cudaSuccess ? LEMC_OK : LEMC_ERR_CUDA;
 }
 
+// Host-side settings of the bounded waits (lemc_debug_gram_wait).
+long long g_wait_cycles = kWaitCycles;
+int g_hold_loads = 0;
+
 }  // namespace
+
+int set_gram_wait(long long cycles, int hold_loads) {
+  if (cycles < 0) return LEMC_ERR_ARG;
+  g_wait_cycles = cycles > 0 ? cycles : kWaitCycles;
+  g_hold_loads = hold_loads != 0;
+  return LEMC_OK;
+}
 
 int launch_gram_tc_rows(const float* V, int ldv, int total_rows, const float* rec_w, int ldw,
                         int Wpad, const TcTile* tiles, int n_jobs, int n_splits, double* partials,
@@ -775,6 +812,8 @@ int launch_gram_tc_rows(const float* V, int ldv, int total_rows, const float* re
   a.flush_every = flush_every > 0 ? flush_every : (tf32 ? 2 : 4);
   a.passes = (mode == LEMC_GRAM_BF16X4) ? 4 : 3;
   a.err = err;
+  a.wait_cycles = g_wait_cycles;
+  a.hold_loads = g_hold_loads;
   return tf32 ? launch_t<true>(a, n_jobs, st) : launch_t<false>(a, n_jobs, st);
 }
 

@@ -17,11 +17,13 @@
 // owns particles l, l+32, ...  The 16 neighbours are found from packed
 // (distance^2, index) keys: each lane sorts its 8 keys once, then 16 rounds
 // of a warp-wide minimum (redux.sync) of the lane heads pop them in ascending
-// order.  Each lane evaluates two of the 64 hidden units of each layer with
-// packed FP32x2 arithmetic; the mean phi features reach all lanes through a
+// order; lane n keeps the n-th neighbour and forms its frame coordinates,
+// which reach every lane by shuffles.  Each lane evaluates two of the 64
+// hidden units of each layer with packed FP32x2 arithmetic; the mean phi features reach all lanes through a
 // per-warp shared-memory buffer; every reduction is an xor butterfly, so all
 // lanes hold bitwise identical values and take the same accept decision.
-// Random numbers: Philox {i, sweep, walker, 4}.
+// Random numbers: Philox {i, sweep, walker, 4}, drawn 32 moves at a time (one
+// move per lane) and broadcast by shuffles.
 //
 // Training (evolution strategies + Adam, forward-only kernels): the objective
 // J = E[min(1, A) |z' - z_i|^2] over (configuration, particle, eps) samples
@@ -122,16 +124,14 @@ __device__ NetOut net_eval(const float* __restrict__ P, const float2* zs, int N,
       key[t] = (__float_as_uint(fmaf(dx, dx, dy * dy)) & 0xFFFFFF00u) | uint32_t(j);
     }
   }
-  // phi for this lane's hidden units lane and lane + 32, as one packed pair
-  const float2 W0X = make_float2(P[kOffW1 + 2 * lane], P[kOffW1 + 2 * (lane + 32)]);
-  const float2 W0Y = make_float2(P[kOffW1 + 2 * lane + 1], P[kOffW1 + 2 * (lane + 32) + 1]);
-  const float2 B0 = make_float2(P[kOffB1 + lane], P[kOffB1 + lane + 32]);
-  float2 g = make_float2(0.f, 0.f);
-  int cnt = 0;
   // The 16 nearest in ascending key order: each lane sorts its keys once, then
-  // every round takes the warp minimum of the lane heads and its lane pops it.
+  // every round takes the warp minimum of the lane heads and its lane pops it;
+  // lane n keeps the n-th neighbour.
   static_assert(kSlots == 8, "sort8 network");
+  static_assert(kNbr <= 32, "one neighbour per lane");
   sort8(key);
+  uint32_t mine = 0xFFFFFFFFu;
+  int cnt = 0;
   for (int n = 0; n < kNbr; ++n) {
     const uint32_t m = __reduce_min_sync(0xffffffffu, key[0]);
     if (m == 0xFFFFFFFFu) break;
@@ -139,12 +139,27 @@ __device__ NetOut net_eval(const float* __restrict__ P, const float2* zs, int N,
 #pragma unroll
     for (int t = 0; t < kSlots - 1; ++t) key[t] = pop ? key[t + 1] : key[t];
     key[kSlots - 1] = pop ? 0xFFFFFFFFu : key[kSlots - 1];
-    const int j = int(m & 0xFFu);
-    const float dx = zs[j].x - zc.x, dy = zs[j].y - zc.y;
-    const float xr = (dx * c + dy * s) * kInScale, xt = (dy * c - dx * s) * kInScale;
-    const float2 h = __ffma2_rn(W0X, make_float2(xr, xr), __ffma2_rn(W0Y, make_float2(xt, xt), B0));
-    g = __fadd2_rn(g, make_float2(fmaxf(h.x, 0.f), fmaxf(h.y, 0.f)));
+    mine = lane == n ? m : mine;
     ++cnt;
+  }
+  // each lane forms the frame coordinates of its own neighbour once; phi then
+  // runs over the neighbours in the same ascending order, their coordinates
+  // broadcast by shuffles, two hidden units per lane as one packed pair
+  float xr = 0.f, xt = 0.f;
+  if (lane < cnt) {
+    const int j = int(mine & 0xFFu);
+    const float dx = zs[j].x - zc.x, dy = zs[j].y - zc.y;
+    xr = (dx * c + dy * s) * kInScale;
+    xt = (dy * c - dx * s) * kInScale;
+  }
+  const float2 W0X = make_float2(P[kOffW1 + 2 * lane], P[kOffW1 + 2 * (lane + 32)]);
+  const float2 W0Y = make_float2(P[kOffW1 + 2 * lane + 1], P[kOffW1 + 2 * (lane + 32) + 1]);
+  const float2 B0 = make_float2(P[kOffB1 + lane], P[kOffB1 + lane + 32]);
+  float2 g = make_float2(0.f, 0.f);
+  for (int n = 0; n < cnt; ++n) {
+    const float a = __shfl_sync(0xffffffffu, xr, n), b = __shfl_sync(0xffffffffu, xt, n);
+    const float2 h = __ffma2_rn(W0X, make_float2(a, a), __ffma2_rn(W0Y, make_float2(b, b), B0));
+    g = __fadd2_rn(g, make_float2(fmaxf(h.x, 0.f), fmaxf(h.y, 0.f)));
   }
   if (cnt > 0) {
     const float inv = 1.f / float(cnt);
@@ -272,12 +287,21 @@ learned_sweep_kernel(const SweepArgs a, const __nv_bfloat16* __restrict__ wts) {
   uint32_t nacc = 0;
   for (int sw = 0; sw < a.n_sweeps; ++sw) {
     const uint32_t sweep = sweep_base + uint32_t(sw);
+    float er_l = 0.f, et_l = 0.f, lu_l = 0.f;
     for (int i = 0; i < N; ++i) {
-      const U4 r = philox4x32_10(U4{uint32_t(i), sweep, uint32_t(w), kTagLearned}, a.seed_lo, a.seed_hi);
-      float er, et;
-      box_muller(r.x, r.y, er, et);
+      // the randoms of move i come from Philox {i, sweep, walker, 4}: lane l
+      // draws those of move 32 b + l for the whole block b of 32 moves
+      if ((i & 31) == 0) {
+        const U4 r = philox4x32_10(U4{uint32_t(i + lane), sweep, uint32_t(w), kTagLearned},
+                                   a.seed_lo, a.seed_hi);
+        box_muller(r.x, r.y, er_l, et_l);
+        lu_l = __logf(u01(r.z));
+      }
+      const float er = __shfl_sync(0xffffffffu, er_l, i & 31);
+      const float et = __shfl_sync(0xffffffffu, et_l, i & 31);
+      const float lu = __shfl_sync(0xffffffffu, lu_l, i & 31);
       const Move mv = propose(P, zs, N, i, a.invR, m, er, et, lane, gsm[wib]);
-      const bool acc = __logf(u01(r.z)) < mv.log_a;
+      const bool acc = lu < mv.log_a;
       __syncwarp();
       if (acc) {
         if (lane == (i & 31)) zs[i] = mv.zn;

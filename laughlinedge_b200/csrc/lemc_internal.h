@@ -89,6 +89,9 @@ int launch_init_walkers(float2* pos, int W, int N, float radius, uint32_t seed_l
 // series_idx (may be null): the walker-mean series goes to series + 8 * *series_idx
 int launch_basis(const float2* rec_p, int W, int K, int N, const BasisProgram& prog, float* V,
                  int ldv, double* series, const uint32_t* series_idx, cudaStream_t st);
+// Bound (cycles, 0 = default) of the contraction's mbarrier waits, and the test
+// hook that keeps its loader from issuing (so that every wait expires).
+int set_gram_wait(long long cycles, int hold_loads);
 // plane[w] = scale * Re p_k[w] (the multipole potential's USER plane)
 int launch_multipole_plane(const float2* rec_p, int W, int K, int k, double scale, float* plane,
                            cudaStream_t st);

@@ -415,6 +415,11 @@ class Sampler:
         check(self.lib.lemc_lanes_per_walker(self._h, C.byref(g)), "lemc_lanes_per_walker")
         return g.value
 
+    def gram_splits(self) -> int:
+        g = C.c_int()
+        check(self.lib.lemc_gram_splits(self._h, C.byref(g)), "lemc_gram_splits")
+        return g.value
+
     def stream(self) -> int:
         h = C.c_void_p()
         check(self.lib.lemc_stream(self._h, C.byref(h)), "lemc_stream")
