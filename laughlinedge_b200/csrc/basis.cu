@@ -88,7 +88,8 @@ basis_kernel(const float2* __restrict__ rec_p, int W, int K, float pN, BasisProg
   // another's column):
   //   ps[k][thread]  = p_k of the thread's walkers, k = 0..K (p_0 = N)
   //   stk[d][thread] = value of the depth-d node on the current DFS path, d < K
-  // followed by the block's program segment and the two nodes after it.
+  // followed by the block's program segment and the two nodes after it, and
+  // their range factors.
   extern __shared__ float4 smem_basis[];
   constexpr int T = kBasisThreads;
   constexpr int R = T * P;  // row stride in float2
@@ -100,8 +101,12 @@ basis_kernel(const float2* __restrict__ rec_p, int W, int K, float pN, BasisProg
   const int t0 = __ldg(prog.seg_dev + blockIdx.y);
   const int t1 = __ldg(prog.seg_dev + blockIdx.y + 1);
   int4* snodes = reinterpret_cast<int4*>(smem_basis) + (2 * K + 1) * R / 2;
-  for (int i = tid; i < t1 - t0 + 2; i += T)
+  float* sscale = reinterpret_cast<float*>(snodes + prog.max_seg + 2);
+  const bool scaled = prog.node_scale != nullptr;
+  for (int i = tid; i < t1 - t0 + 2; i += T) {
     snodes[i] = __ldg(reinterpret_cast<const int4*>(prog.nodes) + t0 + i);
+    if (scaled) sscale[i] = __ldg(prog.node_scale + t0 + i);
+  }
   Vals<P> v0;
 #pragma unroll
   for (int i = 0; i < P; ++i) v0.c[i] = make_float2(pN, 0.f);
@@ -146,6 +151,7 @@ basis_kernel(const float2* __restrict__ rec_p, int W, int K, float pN, BasisProg
   // node = {depth, part, row_re, row_im}; the device array ends with two
   // sentinel nodes {0, 0, -1, -1}, so nodes t + 1 and t + 2 always exist.
   const int4* nodes = snodes - t0;
+  const float* nscale = sscale - t0;
   float* __restrict__ Vw = V + w0;
   Vals<P> one;
 #pragma unroll
@@ -168,8 +174,8 @@ basis_kernel(const float2* __restrict__ rec_p, int W, int K, float pN, BasisProg
     if (descend) vstore<P>(stk + nd.x * R, v);
     if (nd.z >= 0) {
       Vals<P> out = v;
-      if (prog.row_scale) {
-        const float sc = __ldg(prog.row_scale + nd.z);
+      if (scaled) {
+        const float sc = nscale[t];
 #pragma unroll
         for (int i = 0; i < P; ++i) out.c[i] = make_float2(sc * v.c[i].x, sc * v.c[i].y);
       }
@@ -191,7 +197,7 @@ template <int P>
 int launch_p(const float2* rec_p, int W, int K, int N, const BasisProgram& prog, float* V,
              int ldv, double* series, const uint32_t* series_idx, cudaStream_t st) {
   const size_t smem = sizeof(float2) * size_t(2 * K + 1) * kBasisThreads * P +
-                      sizeof(BasisNode) * size_t(prog.max_seg + 2);
+                      (sizeof(BasisNode) + sizeof(float)) * size_t(prog.max_seg + 2);
   if (smem > 40 * 1024) {  // the static reduction buffer shares the 48 KiB default
     if (cudaFuncSetAttribute(basis_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              int(smem)) != cudaSuccess)

@@ -178,7 +178,8 @@ struct lemc_ctx {
   std::vector<double> bin_last;
   uint64_t bin_last_meas = 0;
   std::vector<double> row_scale;      // per basis row
-  DevBuf<float> d_row_scale;          // per V row
+  std::vector<BasisNode> prog_host;   // the basis program (with its sentinels)
+  DevBuf<float> d_node_scale;         // per program node
   bool scale_pending = false;
   bool gram_tune_pending = false;  // autotune the contraction's walker split
   int gram_splits = 0;             // the tuned split (0: one-wave rule)
@@ -304,6 +305,7 @@ int build_program(lemc_ctx* c) {
   }
   prog.push_back({0, 0, -1, -1});  // two sentinels: the kernel reads up to two nodes ahead
   prog.push_back({0, 0, -1, -1});
+  c->prog_host = prog;
   LEMC_TRY(c->prog.alloc(prog.size()));
   LEMC_CUDA(cudaMemcpy(c->prog.p, prog.data(), prog.size() * sizeof(BasisNode),
                        cudaMemcpyHostToDevice));
@@ -710,7 +712,7 @@ int lemc_destroy(lemc_ctx* c) {
   c->d_tc_tiles.release();
   c->d_tc_secs.release();
   c->tc_partials.release();
-  c->d_row_scale.release();
+  c->d_node_scale.release();
   for (auto& e : c->ev)
     if (e) cudaEventDestroy(e);
   for (auto& e : c->pev) cudaEventDestroy(e);
@@ -757,13 +759,13 @@ int lemc_set_sectors(lemc_ctx* c, const int32_t* sectors, int n) {
   LEMC_TRY(build_program(c));
   LEMC_TRY(alloc_records(c));
   c->row_scale.assign(c->D, 1.0);
-  LEMC_TRY(c->d_row_scale.alloc(std::max(1, 2 * c->D)));
+  LEMC_TRY(c->d_node_scale.alloc(c->prog_host.size()));
   {
-    std::vector<float> ones(std::max(1, 2 * c->D), 1.f);
-    LEMC_CUDA(cudaMemcpy(c->d_row_scale.p, ones.data(), sizeof(float) * ones.size(),
+    std::vector<float> ones(c->prog_host.size(), 1.f);
+    LEMC_CUDA(cudaMemcpy(c->d_node_scale.p, ones.data(), sizeof(float) * ones.size(),
                          cudaMemcpyHostToDevice));
   }
-  c->bprog.row_scale = c->d_row_scale.p;
+  c->bprog.node_scale = c->d_node_scale.p;
   c->scale_pending = c->cfg.guide == LEMC_GUIDE_LAUGHLIN;
   c->gram_tune_pending = c->cfg.lanes_per_walker < 0 && c->cfg.guide == LEMC_GUIDE_LAUGHLIN &&
                          c->cfg.gram_mode != LEMC_GRAM_FP64;
@@ -1038,7 +1040,7 @@ static int compute_row_scales(lemc_ctx* c) {
     for (int k = 1; k <= K; ++k)
       lp[size_t(k) * Ws + w] = std::max(-80.0, 0.5 * std::log(re[k] * re[k] + im[k] * im[k]));
   }
-  std::vector<float> dev(2 * size_t(D), 1.f);
+  std::vector<float> vrow(2 * size_t(D), 1.f);  // per V row
   for (int r = 0; r < D; ++r) {
     double mean = 0;
     for (const auto& pp : c->basis.rows[r].pairs) {
@@ -1049,10 +1051,13 @@ static int compute_row_scales(lemc_ctx* c) {
     const double sc = std::min(1e30, std::max(1e-30, std::exp(-mean)));
     const float scf = float(sc);
     c->row_scale[r] = double(scf);  // the factor the kernel applies, exactly
-    dev[c->row_vre[r]] = scf;
-    dev[c->row_vim[r]] = scf;
+    vrow[c->row_vre[r]] = scf;
+    vrow[c->row_vim[r]] = scf;
   }
-  LEMC_CUDA(cudaMemcpyAsync(c->d_row_scale.p, dev.data(), sizeof(float) * dev.size(),
+  std::vector<float> dev(c->prog_host.size(), 1.f);  // per program node
+  for (size_t t = 0; t < dev.size(); ++t)
+    if (c->prog_host[t].row_re >= 0) dev[t] = vrow[c->prog_host[t].row_re];
+  LEMC_CUDA(cudaMemcpyAsync(c->d_node_scale.p, dev.data(), sizeof(float) * dev.size(),
                             cudaMemcpyHostToDevice, c->stream));
   LEMC_CUDA(cudaStreamSynchronize(c->stream));
   return LEMC_OK;

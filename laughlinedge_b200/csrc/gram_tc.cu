@@ -25,19 +25,21 @@
 // read it from there, so shared memory only carries the raw TMA stages and
 // the (weighted, split) B operand.
 //
-// Pipeline (864 threads, one CTA per SM):
-//   warp 25      loader: tiled TMA loads per K-chunk (A panel 128 x KC in
+// Pipeline (608 threads, one CTA per SM):
+//   warp 17      loader: tiled TMA loads per K-chunk (A panel 128 x KC in
 //                128-byte-swizzled boxes of 32 samples, B panel 32 x KC,
 //                weight planes 3 x KC; rows past the end are zero-filled by
 //                the TMA unit) into a ring of raw FP32 stages;
-//   warps 8-15   A converters: thread = A row (TMEM lane) and one half of the
-//                chunk's columns; raw FP32 -> hi/lo, stored to the
-//                tensor-memory A stage with tcgen05.st;
-//   warps 16-23  B converters: raw FP32 -> weighted, split hi/lo B operands in
+//   warps 8-11   A converters: thread = A row (TMEM lane); raw FP32 -> hi/lo,
+//                stored to the tensor-memory A stage with tcgen05.st;
+//   warps 12-15  B converters: raw FP32 -> weighted, split hi/lo B operands in
 //                128-byte-swizzled K-major shared-memory layout;
-//   warp 24      allocates 512 TMEM columns, one lane issues tcgen05.mma;
-//   warp 26      scheduler: makes the issuer's barrier waits and hands each
+//   warp 16      allocates 512 TMEM columns, one lane issues tcgen05.mma;
+//   warp 18      scheduler: makes the issuer's barrier waits and hands each
 //                K-chunk to it through a named barrier;
+// (Doubling the converter warps to 864 threads held the kernel to 72
+// registers and ran slower: 0.321 against 0.266 ms at the mixed-precision
+// workload.)
 //   warps 0-7    epilogue: TMEM lane quarter = warp % 4, column half =
 //                warp / 4, 48 FP32 accumulators per thread.
 // Tensor memory columns: hi*hi buffers at 0 and 128, corrections at 256, A
@@ -64,16 +66,15 @@ constexpr int kOpRowBytes = 128;   // one swizzle-128B row of split operands
 constexpr int kBTileBytes = kN * kOpRowBytes;  // 12 KB
 constexpr int kOpStages = 2;
 constexpr int kEpiWarps = 8;
-constexpr int kAConvWarp0 = 8;     // warps 8-15: A converters (lane quarter = warp % 4,
-                                   // column half = (warp - 8) / 4)
-constexpr int kBConvWarp0 = 16;    // warps 16-23: B converters
-constexpr int kBConvThreads = 8 * 32;
-constexpr int kConvThreads = 16 * 32;
+constexpr int kAConvWarp0 = 8;     // warps 8-11: A converters (lane quarter = warp % 4)
+constexpr int kBConvWarp0 = 12;    // warps 12-15: B converters
+constexpr int kBConvThreads = 4 * 32;
+constexpr int kConvThreads = 8 * 32;
 constexpr int kEpiCols = kN / (kEpiWarps / 4);  // accumulator columns per epilogue thread
-constexpr int kMmaWarp = 24;
-constexpr int kLoadWarp = 25;
-constexpr int kSchedWarp = 26;     // does the issuer's barrier waits (see the MMA issuer)
-constexpr int kThreads = 27 * 32;
+constexpr int kMmaWarp = 16;
+constexpr int kLoadWarp = 17;
+constexpr int kSchedWarp = 18;     // does the issuer's barrier waits (see the MMA issuer)
+constexpr int kThreads = 19 * 32;
 constexpr int kTmemCols = 512;
 constexpr uint32_t kColHH = 0;     // hi*hi buffers at 0 and 128
 constexpr uint32_t kColCorr = 256; // corrections
@@ -410,7 +411,6 @@ gram_tc_kernel(const TcArgs a, const __grid_constant__ CUtensorMap tmA,
     // Thread = A row r = TMEM lane; its raw row segment sits in 128-byte
     // swizzled boxes (16-byte chunk j of row r at r*128 + ((j ^ (r & 7)) << 4)).
     const int quarter = warp & 3;
-    const int half = (warp - kAConvWarp0) >> 2;  // which 16 TMEM columns of the stage
     const int r = quarter * 32 + lane;
     const uint32_t lane_base = uint32_t(quarter * 32) << 16;
     for (int c = 0; c < nch; ++c) {
@@ -420,7 +420,8 @@ gram_tc_kernel(const TcArgs a, const __grid_constant__ CUtensorMap tmA,
       tc_fence_after();
       const uint8_t* raw = sm->raw[rs];
       const uint32_t a_hi = tmem + lane_base + kColA + uint32_t(os * 64);
-      {
+#pragma unroll
+      for (int half = 0; half < 2; ++half) {
         // 16 TMEM columns: TF32 -> 16 samples, BF16 -> 32 samples (2 per column)
         uint32_t hv[16], lv[16];
         if (TF32) {
@@ -459,7 +460,7 @@ gram_tc_kernel(const TcArgs a, const __grid_constant__ CUtensorMap tmA,
       mbar_arrive(&sm->op_full[os]);
       mbar_arrive(&sm->raw_empty[rs]);
     }
-  } else if (warp >= kBConvWarp0 && warp < kBConvWarp0 + 8) {
+  } else if (warp >= kBConvWarp0 && warp < kBConvWarp0 + 4) {
     // ---------------------------- B converters -----------------------------
     const int t = threadIdx.x - kBConvWarp0 * 32;
     for (int c = 0; c < nch; ++c) {

@@ -54,9 +54,10 @@ struct BasisProgram {
   int n_seg = 0;
   int max_seg = 0;  // longest segment, in nodes
   const int* seg_dev = nullptr;  // n_seg + 1 segment starts (node indices), on the device
-  // per-V-row factor applied when a value is stored (the Re and Im rows of a
-  // state carry the same factor); nullptr stores the plain products
-  const float* row_scale = nullptr;
+  // per-node factor applied when a node's value is stored (its state's range
+  // factor; n_nodes + 2 entries with the sentinels); nullptr stores the plain
+  // products
+  const float* node_scale = nullptr;
 };
 
 // One tile of the SIMT FP64 Gram accumulation: three weighted sums

@@ -106,7 +106,11 @@ int main(int argc, char** argv) {
   const float sigma = float(std::atof(argv[6]));
   const long clock0 = std::atol(argv[7]);
   const unsigned blocks = unsigned(std::atoi(argv[8]));
-  const std::string out_path = argv[9];
+  std::string out_path = argv[9];
+  if (!out_path.empty() && out_path[0] != '/') {  // relative to the starting directory
+    char cwd[4096];
+    if (getcwd(cwd, sizeof cwd)) out_path = std::string(cwd) + "/" + out_path;
+  }
   // the reference writes its .tsv files under ../output relative to the
   // working directory
   const std::string work = argc > 10 ? argv[10] : "ref_edge_work/run";

@@ -52,7 +52,7 @@ def cplx(a):
 
 
 def main(outdir):
-    outdir = Path(outdir)
+    outdir = Path(outdir).resolve()
     outdir.mkdir(parents=True, exist_ok=True)
     work = Path("/tmp/ref_edge_work/run")
     reps, burn, samples, blocks = int(sys.argv[2]), int(sys.argv[3]), int(sys.argv[4]), int(sys.argv[5])

@@ -13,9 +13,9 @@ profiler select e.g. the third contraction with ``-k regex:gram_tc -s 2 -c 1``.
 (N=200, m=3, init sigma 0.3, seed 5, untrained weights) and a W-walker context
 (default 4096) that uses it, and runs three single unmeasured sweeps.
 
-``python tests/profile_case.py occupation [walkers]`` runs one occupation
-estimate (N=50, m=3, dL=4, l_cutoff = m(N-1)+15, 50 burn-in + 100 measured
-sweeps; default 65536 walkers).
+``python tests/profile_case.py occupation [walkers] [sweeps]`` runs one
+occupation estimate (N=50, m=3, dL=4, l_cutoff = m(N-1)+15, sweeps/2 burn-in
++ sweeps measured in one launch; defaults 65536 walkers, 100 sweeps).
 """
 from __future__ import annotations
 
@@ -45,8 +45,9 @@ def learned(argv) -> int:
 
 def occ(argv) -> int:
     W = int(argv[0]) if argv else 65536
+    sweeps = int(argv[1]) if len(argv) > 1 else 100
     N, m = 50, 3
-    out, acc = occupation(N, m, 4, m * (N - 1) + 15, W, 100, burn_in=50)
+    out, acc = occupation(N, m, 4, m * (N - 1) + 15, W, sweeps, burn_in=sweeps // 2)
     print("ok", acc, out.shape)
     return 0
 
