@@ -1,10 +1,13 @@
 """Statistical parity of the CUDA estimators with the reference estimator.
 
-The fixture (tests/golden/config1_reference_estimator.json, made by
-make_parity_fixture.py) holds the oracle's restatement of the reference
-estimator -- one chain per basis row guided by |P_a Psi_m|^2 -- at m = 3,
-N = 8, omega = 1e-2, kappa = 1e-4, dL = 1..6: 32 replicas, mean and
-standard deviation of the normalised M and H and of the spectrum.
+Two fixtures hold the reference estimator at m = 3, N = 8, omega = 1e-2,
+kappa = 1e-4, dL = 1..6 (mean and standard deviation over independent
+replicas of the normalised M and H and of the spectrum):
+  config1_reference_run.json        the reference's own sampler
+      (edgeMC::spectrum_compute compiled from its sources, run on a B200 by
+      make_reference_fixture.py; exponent-2 and exponent-4 builds combined);
+  config1_reference_estimator.json  the oracle's C restatement of it
+      (make_parity_fixture.py).
 
 The GPU runs the same physics with (i) the shared Laughlin guide and the
 tcgen05 S/H contraction and (ii) its own port of the per-row reference
@@ -24,9 +27,11 @@ import scipy.linalg as sl
 from scipy import stats
 
 pytestmark = pytest.mark.gpu
-GOLD = json.loads((Path(__file__).resolve().parent / "golden" / "config1_reference_estimator.json").read_text())
-PHY = GOLD["physics"]
+FIXTURES = ["config1_reference_run.json", "config1_reference_estimator.json"]
+_DIR = Path(__file__).resolve().parent / "golden"
+PHY = json.loads((_DIR / FIXTURES[1]).read_text())["physics"]
 SECTORS = [1, 2, 3, 4, 5, 6]
+_OUT = {}
 
 
 FAMILY_ALPHA = 1e-3
@@ -75,11 +80,11 @@ def _welch(g_mean, g_var, n_g, r_mean, r_var, n_r):
     return t, dof
 
 
-def _check(lemc, out, label):
-    R_ref = GOLD["sampling"]["replicas"]
+def _check(lemc, out, label, gold):
+    R_ref = gold["sampling"]["replicas"]
     tests = []  # (what, t, dof)
     for dL in SECTORS:
-        ref = GOLD["sectors"][str(dL)]
+        ref = gold["sectors"][str(dL)]
         reps = len(out[dL]["M"])
         for key in ("M", "H"):
             g = np.array(out[dL][key])
@@ -107,11 +112,22 @@ def _check(lemc, out, label):
         assert t < crit, (label, what, t, dof, crit)
 
 
-def test_laughlin_guide_tc_gram_matches_reference_estimator(lemc, cuda_ctx):
-    out = _gpu_replicas(lemc, lemc._lib.GUIDE_LAUGHLIN, lemc._lib.GRAM_TF32X3)
-    _check(lemc, out, "laughlin+tf32x3")
+def _replicas(lemc, guide):
+    if guide not in _OUT:  # the GPU replicas are shared by both fixtures
+        if guide == lemc._lib.GUIDE_LAUGHLIN:
+            _OUT[guide] = _gpu_replicas(lemc, guide, lemc._lib.GRAM_TF32X3)
+        else:
+            _OUT[guide] = _gpu_replicas(lemc, guide, lemc._lib.GRAM_FP64, W=4096)
+    return _OUT[guide]
 
 
-def test_gpu_reference_estimator_matches_oracle(lemc, cuda_ctx):
-    out = _gpu_replicas(lemc, lemc._lib.GUIDE_ROW, lemc._lib.GRAM_FP64, W=4096)
-    _check(lemc, out, "rows")
+@pytest.mark.parametrize("fixture", FIXTURES)
+def test_laughlin_guide_tc_gram_matches_reference_estimator(lemc, cuda_ctx, fixture):
+    gold = json.loads((_DIR / fixture).read_text())
+    _check(lemc, _replicas(lemc, lemc._lib.GUIDE_LAUGHLIN), "laughlin+tf32x3 vs " + fixture, gold)
+
+
+@pytest.mark.parametrize("fixture", FIXTURES)
+def test_gpu_reference_estimator_matches_reference(lemc, cuda_ctx, fixture):
+    gold = json.loads((_DIR / fixture).read_text())
+    _check(lemc, _replicas(lemc, lemc._lib.GUIDE_ROW), "rows vs " + fixture, gold)
