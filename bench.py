@@ -228,17 +228,44 @@ def tau_value(t):
     return None
 
 
+def reference_cuda_sampler(N):
+    """The reference's own CUDA sampler (edgeMC::spectrum_compute, compiled from
+    its sources for sm_100a by oracle/Makefile into oracle/_ref) timed on this
+    GPU by its own cudaEvents around the row launch (em_spectrum.cu:273-287):
+    one basis row (dL = 1) of its default grid, 32 x 128 walkers, 100 burn-in
+    + 200 measured sweeps.  None when the build or a GPU is absent."""
+    exe = ROOT / "oracle" / "_ref" / ("ref_edge200_e2" if N == 200 else "ref_edge_e2")
+    if not exe.exists():
+        return None
+    with tempfile.TemporaryDirectory() as tmp:
+        out = Path(tmp) / "ref.json"
+        try:
+            subprocess.run([str(exe), "spectrum", "1", "100", "200", "1", "0.3", "4242", "32",
+                            str(out), str(Path(tmp) / "run")], check=True, timeout=600,
+                           stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+            d = json.loads(out.read_text())
+        except Exception as exc:  # reported, never required
+            return {"error": str(exc)}
+    ms = d["runs"][0]["kernel_ms"]
+    return {"walker_sweeps_per_s_per_row": d["walkers"] * 300 / (sum(ms) * 1e-3),
+            "kernel_ms_per_row": sum(ms) / len(ms), "particles": d["particles"],
+            "walkers": d["walkers"], "sweeps_per_launch": 300,
+            "note": "the reference's mcmc_hamiltonian, one basis row per launch; our "
+                    "walker-sweep covers every row of every sector"}
+
+
 def run_reference(args, ws, rank):
     if rank != 0:
         return
     w = MIXED if args.mixed else WORKLOAD
     cb = cpu_port(w)
+    rc = reference_cuda_sampler(w["particles"])
     line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT,
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
             "config": {k: w[k] for k in ("workload", "particles", "inverse_filling", "walkers")},
-            "cpu_baseline": cb,
+            "cpu_baseline": cb, "reference_cuda_sampler": rc,
             "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
