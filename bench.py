@@ -143,11 +143,13 @@ def dist_init():
 def allreduce_max(x, ws):
     if ws == 1:
         return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from laughlinedge_b200.replicas import max_over_ranks
+    return max_over_ranks(x)
+
+
+def rank_seed(seed, rank):
+    from laughlinedge_b200.replicas import rank_seed as rs
+    return rs(seed, rank)
 
 
 def gram_mode_id(name):
@@ -398,7 +400,7 @@ def run_ours(args, ws, rank, local):
     torch.cuda.set_device(local)
     N, m, W = w["particles"], w["inverse_filling"], w["walkers"]
     mode = gram_mode_id(args.gram or w["gram_mode"])
-    seed = w["seed"] + 1000003 * rank
+    seed = rank_seed(w["seed"], rank)
     sectors = w["sectors"]
     gb = args.graph_batch
 
@@ -570,7 +572,7 @@ def run_mixed(args, ws, rank, local):
     torch.cuda.set_device(local)
     N, m, W = w["particles"], w["inverse_filling"], w["walkers"]
     mode = gram_mode_id(args.gram or w["gram_mode"])
-    seed = w["seed"] + 1000003 * rank
+    seed = rank_seed(w["seed"], rank)
     p0 = L.Sampler(L.SamplerConfig(N, m, W, step_sigma=w["sigma"], seed=seed, lanes_per_walker=-1),
                    [1, 2, 3, 4])
     p0.init_walkers()
