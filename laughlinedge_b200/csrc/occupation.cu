@@ -147,13 +147,28 @@ __global__ void __launch_bounds__(kOccThreads) occupation_kernel(const OccArgs a
       sincospif(2.f * u01(r.y), &sn, &cs);
       const float2 zo = Z(i);
       const float2 zn = make_float2(zo.x + sigma * (rad * cs), zo.y + sigma * (rad * sn));
-      // Jastrow log|ratio| over the shared particles 1..N-1
+      // Jastrow log|ratio| over the shared particles 1..N-1: FP32 products of
+      // the squared distances, four terms at a time (at most 1e+-16 for any
+      // distance between 1e-4 and 1e4), one log2 of each product per chunk,
+      // accumulated in FP64
       double lj = 0.0;
-      for (int j = 1; j < N; ++j) {
-        if (j == i) continue;
-        const float2 zj = Z(j);
-        const float dx = zn.x - zj.x, dy = zn.y - zj.y, ex = zo.x - zj.x, ey = zo.y - zj.y;
-        lj += 0.5 * (log(double(dx * dx + dy * dy)) - log(double(ex * ex + ey * ey)));
+      {
+        float pn = 1.f, po = 1.f;
+        int c = 0;
+        for (int j = 1; j < N; ++j) {
+          if (j == i) continue;
+          const float2 zj = Z(j);
+          const float dx = zn.x - zj.x, dy = zn.y - zj.y, ex = zo.x - zj.x, ey = zo.y - zj.y;
+          pn *= fmaf(dx, dx, dy * dy);
+          po *= fmaf(ex, ex, ey * ey);
+          if (++c == 4) {
+            lj += double(__log2f(pn) - __log2f(po));
+            pn = po = 1.f;
+            c = 0;
+          }
+        }
+        if (c) lj += double(__log2f(pn) - __log2f(po));
+        lj *= 0.5 * 0.6931471805599453;  // ln|z' - z_j| - ln|z - z_j| summed
       }
       const double gz = double(zo.x) * zo.x + double(zo.y) * zo.y - (double(zn.x) * zn.x + double(zn.y) * zn.y);
       double delta;
