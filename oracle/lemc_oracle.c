@@ -144,8 +144,9 @@ static double guide_log_norm(const cx* gp, const int* gk, const int* gr, int np)
  * with np = 0 for the Laughlin guide.  Returns accepted moves. */
 static uint32_t walker_sweeps(float* pos, int N, int m, double sigma, uint32_t k0, uint32_t k1,
                               uint32_t w, uint32_t sweep0, int n_sweeps, double invR,
-                              const int* gk, const int* gr, int np) {
+                              const int* gk, const int* gr, int np, double* margin) {
   uint32_t acc = 0;
+  if (margin) *margin = INFINITY;
   cx gp[ORC_MAXGP];
   for (int s = 0; s < n_sweeps; ++s) {
     const uint32_t sweep = sweep0 + (uint32_t)s;
@@ -188,6 +189,7 @@ static uint32_t walker_sweeps(float* pos, int N, int m, double sigma, uint32_t k
         }
         delta += guide_log_norm(gnew, gk, gr, np) - before;
       }
+      if (margin && fabs(delta - log(u3)) < *margin) *margin = fabs(delta - log(u3));
       if (delta >= log(u3)) {
         pos[2 * i] = nx;
         pos[2 * i + 1] = ny;
@@ -201,9 +203,25 @@ static uint32_t walker_sweeps(float* pos, int N, int m, double sigma, uint32_t k
 
 /* Advance W walkers.  guide_pairs: [rows][2*ORC_MAXGP] (part, mult) and
  * guide_np[rows]; walker_row == NULL selects the Laughlin guide. */
+/* As orc_sweep; min_margin[w] (may be NULL) receives the smallest
+ * |ln A - ln u| of walker w's moves: the closest its accept decisions came to a
+ * tie, which is where a GPU path that forms ln A in FP32 may decide otherwise. */
+void orc_sweep_margin(float* pos, int W, int N, int m, double sigma, uint64_t seed,
+                      uint32_t sweep0, int n_sweeps, double invR, const int* walker_row,
+                      const int* guide_pairs, const int* guide_np, uint32_t* accepted,
+                      double* min_margin, int nthreads);
+
 void orc_sweep(float* pos, int W, int N, int m, double sigma, uint64_t seed, uint32_t sweep0,
                int n_sweeps, double invR, const int* walker_row, const int* guide_pairs,
                const int* guide_np, uint32_t* accepted, int nthreads) {
+  orc_sweep_margin(pos, W, N, m, sigma, seed, sweep0, n_sweeps, invR, walker_row, guide_pairs,
+                   guide_np, accepted, NULL, nthreads);
+}
+
+void orc_sweep_margin(float* pos, int W, int N, int m, double sigma, uint64_t seed,
+                      uint32_t sweep0, int n_sweeps, double invR, const int* walker_row,
+                      const int* guide_pairs, const int* guide_np, uint32_t* accepted,
+                      double* min_margin, int nthreads) {
   const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
 #ifdef _OPENMP
   if (nthreads > 0) omp_set_num_threads(nthreads);
@@ -220,7 +238,8 @@ void orc_sweep(float* pos, int W, int N, int m, double sigma, uint64_t seed, uin
       }
     }
     const uint32_t a = walker_sweeps(pos + (size_t)w * N * 2, N, m, sigma, k0, k1, (uint32_t)w,
-                                     sweep0, n_sweeps, invR, gk, gr, np);
+                                     sweep0, n_sweeps, invR, gk, gr, np,
+                                     min_margin ? min_margin + w : NULL);
     if (accepted) accepted[w] += a;
   }
 }
@@ -336,11 +355,11 @@ static void run_common(int mode, int N, int m, int W, double sigma, uint64_t see
       }
     }
     float* z = pos + (size_t)w * N * 2;
-    walker_sweeps(z, N, m, sigma, k0, k1, (uint32_t)w, 0u, n_burn, invR, gk, gr, np);
+    walker_sweeps(z, N, m, sigma, k0, k1, (uint32_t)w, 0u, n_burn, invR, gk, gr, np, NULL);
     double rp[2 * ORC_MAXK], rw[6];
     cx v[4096];
     for (int s = 0; s < n_meas; ++s) {
-      walker_sweeps(z, N, m, sigma, k0, k1, (uint32_t)w, (uint32_t)(n_burn + s), 1, invR, gk, gr, np);
+      walker_sweeps(z, N, m, sigma, k0, k1, (uint32_t)w, (uint32_t)(n_burn + s), 1, invR, gk, gr, np, NULL);
       orc_measure(z, 1, N, K, invR, 0, rp, rw);
       if (pser)
         for (int q = 0; q < 8 && q < 2 * K; ++q) pser[((size_t)tid * n_meas + s) * 8 + q] += rp[q];

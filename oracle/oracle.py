@@ -83,21 +83,25 @@ def init_walkers(W, N, radius, seed):
 
 
 def sweep(pos, m, sigma, seed, sweep0, n_sweeps, R, rows=None, walker_row=None, accepted=None,
-          nthreads=0):
-    """Advance positions in place (float32 [W, N, 2]); returns accepted counts."""
+          nthreads=0, margins=None):
+    """Advance positions in place (float32 [W, N, 2]); returns accepted counts.
+    margins (float64 [W], optional) receives each walker's smallest
+    |ln A - ln u| over its moves."""
     lib = load()
     W, N = pos.shape[0], pos.shape[1]
     acc = np.zeros(W, np.uint32) if accepted is None else accepted
+    mg = None if margins is None else _p(margins)
     if rows is not None:
         gp, gn = _guide_arrays(rows)
         wr = np.ascontiguousarray(walker_row, dtype=np.int32)
-        lib.orc_sweep(_p(pos), C.c_int(W), C.c_int(N), C.c_int(m), C.c_double(sigma),
-                      C.c_uint64(seed), C.c_uint32(sweep0), C.c_int(n_sweeps), C.c_double(1.0 / R),
-                      _p(wr), _p(gp), _p(gn), _p(acc), C.c_int(nthreads))
+        lib.orc_sweep_margin(_p(pos), C.c_int(W), C.c_int(N), C.c_int(m), C.c_double(sigma),
+                             C.c_uint64(seed), C.c_uint32(sweep0), C.c_int(n_sweeps),
+                             C.c_double(1.0 / R), _p(wr), _p(gp), _p(gn), _p(acc), mg,
+                             C.c_int(nthreads))
     else:
-        lib.orc_sweep(_p(pos), C.c_int(W), C.c_int(N), C.c_int(m), C.c_double(sigma),
-                      C.c_uint64(seed), C.c_uint32(sweep0), C.c_int(n_sweeps), C.c_double(1.0 / R),
-                      None, None, None, _p(acc), C.c_int(nthreads))
+        lib.orc_sweep_margin(_p(pos), C.c_int(W), C.c_int(N), C.c_int(m), C.c_double(sigma),
+                             C.c_uint64(seed), C.c_uint32(sweep0), C.c_int(n_sweeps),
+                             C.c_double(1.0 / R), None, None, None, _p(acc), mg, C.c_int(nthreads))
     return acc
 
 
