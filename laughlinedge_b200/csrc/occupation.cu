@@ -31,7 +31,6 @@
 namespace lemc {
 namespace {
 
-constexpr int kOccThreads = 64;
 constexpr uint32_t kTagOccMove = 2u, kTagOccInit = 3u;
 
 struct OccArgs {
@@ -89,118 +88,167 @@ __device__ __forceinline__ double guide_arg(const Guide& g) {
   return a;
 }
 
-__global__ void __launch_bounds__(kOccThreads) occupation_kernel(const OccArgs a) {
-  extern __shared__ float2 zsm[];
+// G lanes per walker (one walker group of G consecutive lanes of a warp):
+// lane gl owns the shared particles j = 1 + gl + tG of the Jastrow sums, the
+// estimator's partial products over the same particles and the orbitals
+// l = gl + tG of the estimator; xor-butterfly reductions within the group give
+// every lane bit-identical sums, hence the same accept decision.  Every
+// shuffle sits in control flow that is uniform over the warp (the guide loops
+// run over all kMaxGuideParts slots, the walkers beyond W compute and do not
+// write), so full-warp masks are exact.
+constexpr int kOccLanesThreads = 128;
+
+template <int G>
+__device__ __forceinline__ double group_sum(double v) {
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o, G);
+  return v;
+}
+
+template <int G>
+__device__ __forceinline__ float group_sumf(float v) {
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o, G);
+  return v;
+}
+
+// power sums of the guide parts over particles [j0, j1) of the walker, every
+// lane of the group ending with the same values
+template <int G>
+__device__ __forceinline__ void guide_refresh(Guide& g, const float2* zs, int j0, int j1, float invR,
+                                              int gl) {
+#pragma unroll
+  for (int q = 0; q < kMaxGuideParts; ++q) {
+    double re = 0.0, im = 0.0;
+    if (q < g.n && g.k[q] > 0)
+      for (int j = j0 + gl; j < j1; j += G) {
+        const double2 v = cpow_d(make_double2(zs[j].x * invR, zs[j].y * invR), g.k[q]);
+        re += v.x;
+        im += v.y;
+      }
+    g.p[q] = make_double2(group_sum<G>(re), group_sum<G>(im));
+  }
+}
+
+template <int G>
+__global__ void __launch_bounds__(kOccLanesThreads) occupation_kernel(const OccArgs a) {
+  extern __shared__ double occ_smem[];
+  constexpr int WPB = kOccLanesThreads / G;
   const int t = threadIdx.x;
-  const int w = blockIdx.x * kOccThreads + t;
+  const int gl = t % G, wl = t / G;
+  const int w = blockIdx.x * WPB + wl;
   const bool live = w < a.W;
   const int N = a.N, NP = a.N + 1;
-  auto Z = [&](int j) -> float2& { return zsm[j * kOccThreads + t]; };
+  // ln(l!) for the estimator's orbitals, then the walkers' positions
+  double* lnfact = occ_smem;
+  float2* zs = reinterpret_cast<float2*>(occ_smem + a.Lc) + size_t(wl) * NP;
+  for (int l = t; l < a.Lc; l += kOccLanesThreads) lnfact[l] = lgamma(double(l) + 1.0);
 
-  const int pair = live ? int((int64_t(w) * a.D * a.D) / a.W) : 0;
+  const int wr = live ? w : a.W - 1;  // walkers beyond W compute, never write
+  const int pair = int((int64_t(wr) * a.D * a.D) / a.W);
   const int rowL = pair / a.D, rowR = pair % a.D;
-  Guide gl, gr;
-  gl.n = a.npairs[rowL];
-  gr.n = a.npairs[rowR];
+  Guide gL, gR;
+  gL.n = a.npairs[rowL];
+  gR.n = a.npairs[rowR];
   for (int q = 0; q < kMaxGuideParts; ++q) {
-    gl.k[q] = q < gl.n ? a.pairs[rowL * 2 * kMaxGuideParts + 2 * q] : 0;
-    gl.r[q] = q < gl.n ? a.pairs[rowL * 2 * kMaxGuideParts + 2 * q + 1] : 0;
-    gr.k[q] = q < gr.n ? a.pairs[rowR * 2 * kMaxGuideParts + 2 * q] : 0;
-    gr.r[q] = q < gr.n ? a.pairs[rowR * 2 * kMaxGuideParts + 2 * q + 1] : 0;
+    gL.k[q] = q < gL.n ? a.pairs[rowL * 2 * kMaxGuideParts + 2 * q] : 0;
+    gL.r[q] = q < gL.n ? a.pairs[rowL * 2 * kMaxGuideParts + 2 * q + 1] : 0;
+    gR.k[q] = q < gR.n ? a.pairs[rowR * 2 * kMaxGuideParts + 2 * q] : 0;
+    gR.r[q] = q < gR.n ? a.pairs[rowR * 2 * kMaxGuideParts + 2 * q + 1] : 0;
   }
   // initial positions: uniform in the disk of radius sqrt(2 m N)
   const float r0 = sqrtf(2.f * a.m * N);
-  for (int j = 0; j < NP; ++j) {
+  for (int j = gl; j < NP; j += G) {
     const U4 r = philox4x32_10(U4{uint32_t(j), 0u, uint32_t(w), kTagOccInit}, a.k0, a.k1);
     const float rho = r0 * sqrtf(u01(r.x));
     float sn, cs;
     sincospif(2.f * u01(r.y), &sn, &cs);
-    Z(j) = make_float2(rho * cs, rho * sn);
+    zs[j] = make_float2(rho * cs, rho * sn);
   }
+  __syncthreads();
   uint32_t nacc = 0;
   const float sigma = a.sigma;
   const double mm = double(a.m);
   for (int s = 0; s < a.burn + a.sweeps; ++s) {
     // refresh guide power sums: left over 0..N-1, right over 1..N
-    for (int q = 0; q < gl.n; ++q) {
-      gl.p[q] = make_double2(0.0, 0.0);
-      if (gl.k[q] > 0)
-        for (int j = 0; j < N; ++j) {
-          const double2 v = cpow_d(make_double2(Z(j).x * a.invR, Z(j).y * a.invR), gl.k[q]);
-          gl.p[q].x += v.x;
-          gl.p[q].y += v.y;
-        }
-    }
-    for (int q = 0; q < gr.n; ++q) {
-      gr.p[q] = make_double2(0.0, 0.0);
-      if (gr.k[q] > 0)
-        for (int j = 1; j <= N; ++j) {
-          const double2 v = cpow_d(make_double2(Z(j).x * a.invR, Z(j).y * a.invR), gr.k[q]);
-          gr.p[q].x += v.x;
-          gr.p[q].y += v.y;
-        }
-    }
+    guide_refresh<G>(gL, zs, 0, N, a.invR, gl);
+    guide_refresh<G>(gR, zs, 1, NP, a.invR, gl);
+    float dx_l = 0.f, dy_l = 0.f;
+    double lu_l = 0.0;
     for (int i = 0; i < NP; ++i) {
-      const U4 r = philox4x32_10(U4{uint32_t(i), uint32_t(s), uint32_t(w), kTagOccMove}, a.k0, a.k1);
-      const float rad = sqrtf(-2.f * logf(u01(r.x)));
-      float sn, cs;
-      sincospif(2.f * u01(r.y), &sn, &cs);
-      const float2 zo = Z(i);
-      const float2 zn = make_float2(zo.x + sigma * (rad * cs), zo.y + sigma * (rad * sn));
+      // the randoms of move i, Philox {i, sweep, walker, 2}: lane gl draws
+      // those of move i0 + gl for the block of G moves starting at i0
+      if (i % G == 0) {
+        const U4 r = philox4x32_10(U4{uint32_t(i + gl), uint32_t(s), uint32_t(w), kTagOccMove},
+                                   a.k0, a.k1);
+        const float rad = sqrtf(-2.f * logf(u01(r.x)));
+        float sn, cs;
+        sincospif(2.f * u01(r.y), &sn, &cs);
+        dx_l = sigma * (rad * cs);
+        dy_l = sigma * (rad * sn);
+        lu_l = log(double(u01(r.z)));
+      }
+      const float ddx = __shfl_sync(0xffffffffu, dx_l, i % G, G);
+      const float ddy = __shfl_sync(0xffffffffu, dy_l, i % G, G);
+      const double lu = __shfl_sync(0xffffffffu, lu_l, i % G, G);
+      const float2 zo = zs[i];
+      const float2 zn = make_float2(zo.x + ddx, zo.y + ddy);
       // Jastrow log|ratio| over the shared particles 1..N-1: FP32 products of
-      // the squared distances, four terms at a time (at most 1e+-16 for any
-      // distance between 1e-4 and 1e4), one log2 of each product per chunk,
-      // accumulated in FP64
-      double lj = 0.0;
+      // the squared distances, four terms at a time, one log2 per product
+      float lj2 = 0.f;
       {
         float pn = 1.f, po = 1.f;
         int c = 0;
-        for (int j = 1; j < N; ++j) {
+        for (int j = 1 + gl; j < N; j += G) {
           if (j == i) continue;
-          const float2 zj = Z(j);
+          const float2 zj = zs[j];
           const float dx = zn.x - zj.x, dy = zn.y - zj.y, ex = zo.x - zj.x, ey = zo.y - zj.y;
           pn *= fmaf(dx, dx, dy * dy);
           po *= fmaf(ex, ex, ey * ey);
           if (++c == 4) {
-            lj += double(__log2f(pn) - __log2f(po));
+            lj2 += __log2f(pn) - __log2f(po);
             pn = po = 1.f;
             c = 0;
           }
         }
-        if (c) lj += double(__log2f(pn) - __log2f(po));
-        lj *= 0.5 * 0.6931471805599453;  // ln|z' - z_j| - ln|z - z_j| summed
+        if (c) lj2 += __log2f(pn) - __log2f(po);
       }
+      const double lj = 0.5 * 0.6931471805599453 * double(group_sumf<G>(lj2));
       const double gz = double(zo.x) * zo.x + double(zo.y) * zo.y - (double(zn.x) * zn.x + double(zn.y) * zn.y);
       double delta;
       double2 pl[kMaxGuideParts], pr[kMaxGuideParts];
       if (i == 0) {
-        delta = mm * lj + guide_delta(gl, zo, zn, a.invR, pl) + 0.25 * gz;
+        delta = mm * lj + guide_delta(gL, zo, zn, a.invR, pl) + 0.25 * gz;
       } else if (i == N) {
-        delta = mm * lj + guide_delta(gr, zo, zn, a.invR, pr) + 0.25 * gz;
+        delta = mm * lj + guide_delta(gR, zo, zn, a.invR, pr) + 0.25 * gz;
       } else {
-        const float2 z0 = Z(0), zN = Z(N);
+        const float2 z0 = zs[0], zN = zs[N];
         const double c0 = 0.5 * (log(double((zn.x - z0.x) * (zn.x - z0.x) + (zn.y - z0.y) * (zn.y - z0.y))) -
                                  log(double((zo.x - z0.x) * (zo.x - z0.x) + (zo.y - z0.y) * (zo.y - z0.y))));
         const double cN = 0.5 * (log(double((zn.x - zN.x) * (zn.x - zN.x) + (zn.y - zN.y) * (zn.y - zN.y))) -
                                  log(double((zo.x - zN.x) * (zo.x - zN.x) + (zo.y - zN.y) * (zo.y - zN.y))));
-        delta = mm * (c0 + cN) + guide_delta(gl, zo, zn, a.invR, pl) +
-                guide_delta(gr, zo, zn, a.invR, pr) + 2.0 * mm * lj + 0.5 * gz;
+        delta = mm * (c0 + cN) + guide_delta(gL, zo, zn, a.invR, pl) +
+                guide_delta(gR, zo, zn, a.invR, pr) + 2.0 * mm * lj + 0.5 * gz;
       }
-      if (delta >= log(double(u01(r.z)))) {
-        Z(i) = zn;
+      const bool acc = delta >= lu;
+      __syncwarp();
+      if (acc) {
+        if (gl == 0) zs[i] = zn;
         ++nacc;
         if (i < N)
-          for (int q = 0; q < gl.n; ++q) gl.p[q] = pl[q];
+          for (int q = 0; q < gL.n; ++q) gL.p[q] = pl[q];
         if (i > 0)
-          for (int q = 0; q < gr.n; ++q) gr.p[q] = pr[q];
+          for (int q = 0; q < gR.n; ++q) gR.p[q] = pr[q];
       }
+      __syncwarp();
     }
-    if (s < a.burn || !live) continue;
-    // estimator
-    const float2 z0 = Z(0), zN = Z(N);
+    if (s < a.burn) continue;
+    // estimator: u = prod_{i=1}^{N-1} (z_i - z_N) conj(z_0 - z_i), kept at unit
+    // modulus, as group partial products combined by the butterfly
+    const float2 z0 = zs[0], zN = zs[N];
     double2 u = make_double2(1.0, 0.0);
-    for (int i = 1; i < N; ++i) {
-      const float2 zi = Z(i);
+    for (int i = 1 + gl; i < N; i += G) {
+      const float2 zi = zs[i];
       const double2 num = make_double2(zi.x - zN.x, zi.y - zN.y);
       const double2 den = make_double2(z0.x - zi.x, z0.y - zi.y);
       u = cmul(u, make_double2(num.x * den.x + num.y * den.y, num.y * den.x - num.x * den.y));
@@ -210,16 +258,28 @@ __global__ void __launch_bounds__(kOccThreads) occupation_kernel(const OccArgs a
         u.y /= nu;
       }
     }
-    const double phase = guide_arg(gr) - guide_arg(gl) + mm * atan2(u.y, u.x);
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) {
+      const double2 v = make_double2(__shfl_xor_sync(0xffffffffu, u.x, o, G),
+                                     __shfl_xor_sync(0xffffffffu, u.y, o, G));
+      u = cmul(u, v);
+      const double nu = sqrt(u.x * u.x + u.y * u.y);
+      if (nu > 0) {
+        u.x /= nu;
+        u.y /= nu;
+      }
+    }
+    const double phase = guide_arg(gR) - guide_arg(gL) + mm * atan2(u.y, u.x);
     const double2 q0 = make_double2(0.5 * (double(z0.x) * zN.x + double(z0.y) * zN.y),
                                     0.5 * (double(z0.y) * zN.x - double(z0.x) * zN.y));  // z0 conj(zN) / 2
     const double lx = 0.5 * log(q0.x * q0.x + q0.y * q0.y);
     const double phi = atan2(q0.y, q0.x);
     const double base = -0.25 * (double(z0.x) * z0.x + double(z0.y) * z0.y + double(zN.x) * zN.x +
                                  double(zN.y) * zN.y) - log(2.0 * 3.14159265358979323846);
-    double la = base;  // log magnitude of term l (log of 1/(2 pi l!) folded in)
-    for (int l = 0; l < a.Lc; ++l) {
-      if (l > 0) la += lx - log(double(l));
+    if (!live) continue;
+    for (int l = gl; l < a.Lc; l += G) {
+      // log magnitude of term l: base + l ln|z_0 conj(z_N)/2| - ln l!
+      const double la = base + double(l) * lx - lnfact[l];
       if (la > -700.0) {
         const double mag = exp(la);
         double sn2, cs2;
@@ -230,7 +290,41 @@ __global__ void __launch_bounds__(kOccThreads) occupation_kernel(const OccArgs a
       }
     }
   }
-  if (live) a.accepted[w] = nacc;
+  if (live && gl == 0) a.accepted[w] = nacc;
+}
+
+// Lanes per walker for N + 1 particles: about eight particles per lane.
+int occupation_lanes(int N) {
+  int G = 4;
+  while (G < 32 && (N + G - 1) / G > 8) G *= 2;
+  return G;
+}
+
+size_t occupation_smem(int N, int Lc) {
+  const int G = occupation_lanes(N);
+  return sizeof(double) * size_t(Lc) + sizeof(float2) * size_t(kOccLanesThreads / G) * (N + 1);
+}
+
+template <int G>
+int launch_occ_g(const OccArgs& a, cudaStream_t st) {
+  const size_t smem = occupation_smem(a.N, a.Lc);
+  if (smem > 48 * 1024 &&
+      cudaFuncSetAttribute(occupation_kernel<G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           int(smem)) != cudaSuccess)
+    return LEMC_ERR_CUDA;
+  constexpr int WPB = kOccLanesThreads / G;
+  occupation_kernel<G><<<(a.W + WPB - 1) / WPB, kOccLanesThreads, smem, st>>>(a);
+  return cudaPeekAtLastError() == cudaSuccess ? LEMC_OK : LEMC_ERR_CUDA;
+}
+
+int launch_occupation(const OccArgs& a, cudaStream_t st) {
+  if (occupation_smem(a.N, a.Lc) > 227 * 1024) return LEMC_ERR_CAPACITY;
+  switch (occupation_lanes(a.N)) {
+    case 4: return launch_occ_g<4>(a, st);
+    case 8: return launch_occ_g<8>(a, st);
+    case 16: return launch_occ_g<16>(a, st);
+    default: return launch_occ_g<32>(a, st);
+  }
 }
 
 __global__ void occupation_reduce(const double2* acc, int W, int D, int Lc, double2* out) {
@@ -258,8 +352,7 @@ extern "C" int lemc_occupation(const lemc_occupation_config* cfg, double* out, d
   if (N < 2 || m < 1 || W < 1 || Lc < 1 || cfg->dL < 0 || cfg->dL > kMaxDegree || cfg->sweeps < 1 ||
       cfg->burn_in < 0 || !(cfg->step_sigma > 0.f))
     return LEMC_ERR_ARG;
-  const size_t smem = size_t(kOccThreads) * (N + 1) * sizeof(float2);
-  if (smem > 227 * 1024) return LEMC_ERR_CAPACITY;
+  if (occupation_smem(N, Lc) > 227 * 1024) return LEMC_ERR_CAPACITY;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
     cudaGetLastError();
@@ -313,11 +406,9 @@ extern "C" int lemc_occupation(const lemc_occupation_config* cfg, double* out, d
     a.npairs = d_np;
     a.acc = d_acc;
     a.accepted = d_accp;
-    if (smem > 48 * 1024)
-      ok(cudaFuncSetAttribute(occupation_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     if (st == LEMC_OK) {
-      occupation_kernel<<<(W + kOccThreads - 1) / kOccThreads, kOccThreads, smem>>>(a);
-      ok(cudaPeekAtLastError());
+      const int ls = launch_occupation(a, nullptr);
+      if (ls != LEMC_OK && st == LEMC_OK) st = ls;
       occupation_reduce<<<dim3((Lc + 127) / 128, D * D), 128>>>(d_acc, W, D, Lc, d_out);
       ok(cudaPeekAtLastError());
       ok(cudaDeviceSynchronize());
@@ -407,8 +498,7 @@ extern "C" int lemc_occupation_static(const lemc_occupation_config* cfg, double*
   if (N < 2 || m < 1 || W < 1 || Lc < 1 || cfg->dL < 0 || cfg->dL > kMaxDegree || cfg->sweeps < 1 ||
       cfg->burn_in < 0 || !(cfg->step_sigma > 0.f))
     return LEMC_ERR_ARG;
-  const size_t smem = size_t(kOccThreads) * (N + 1) * sizeof(float2);
-  if (smem > 227 * 1024) return LEMC_ERR_CAPACITY;
+  if (occupation_smem(N, Lc) > 227 * 1024) return LEMC_ERR_CAPACITY;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
     cudaGetLastError();
@@ -469,11 +559,9 @@ extern "C" int lemc_occupation_static(const lemc_occupation_config* cfg, double*
     a.npairs = d_table + size_t(D) * 2 * kMaxGuideParts;
     a.acc = d_acc;
     a.accepted = d_accp;
-    if (smem > 48 * 1024)
-      ok(cudaFuncSetAttribute(occupation_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     if (st == LEMC_OK) {
-      occupation_kernel<<<(W + kOccThreads - 1) / kOccThreads, kOccThreads, smem>>>(a);
-      ok(cudaPeekAtLastError());
+      const int ls = launch_occupation(a, nullptr);
+      if (ls != LEMC_OK && st == LEMC_OK) st = ls;
       occupation_reduce<<<dim3((Lc + 127) / 128, D * D), 128>>>(d_acc, W, D, Lc, d_out);
       ok(cudaPeekAtLastError());
       ok(cudaDeviceSynchronize());
