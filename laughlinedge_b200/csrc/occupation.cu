@@ -75,8 +75,12 @@ __device__ __forceinline__ double guide_delta(const Guide& g, float2 zo, float2 
     const double2 a = cpow_d(wo, g.k[q]), b = cpow_d(wn, g.k[q]);
     pn[q].x += b.x - a.x;
     pn[q].y += b.y - a.y;
-    d += 0.5 * g.r[q] * (log(pn[q].x * pn[q].x + pn[q].y * pn[q].y) -
-                         log(g.p[q].x * g.p[q].x + g.p[q].y * g.p[q].y));
+    // ln of the ratio of squared moduli: formed in FP64, its log in FP32
+    // (the ratio of two moduli of the same power sum before and after one
+    // particle moved; an infinite or zero ratio gives +-inf as the FP64 log did)
+    const double ratio = (pn[q].x * pn[q].x + pn[q].y * pn[q].y) /
+                         (g.p[q].x * g.p[q].x + g.p[q].y * g.p[q].y);
+    d += 0.5 * 0.6931471805599453 * g.r[q] * double(__log2f(float(ratio)));
   }
   return d;
 }
@@ -223,10 +227,14 @@ __global__ void __launch_bounds__(kOccLanesThreads) occupation_kernel(const OccA
         delta = mm * lj + guide_delta(gR, zo, zn, a.invR, pr) + 0.25 * gz;
       } else {
         const float2 z0 = zs[0], zN = zs[N];
-        const double c0 = 0.5 * (log(double((zn.x - z0.x) * (zn.x - z0.x) + (zn.y - z0.y) * (zn.y - z0.y))) -
-                                 log(double((zo.x - z0.x) * (zo.x - z0.x) + (zo.y - z0.y) * (zo.y - z0.y))));
-        const double cN = 0.5 * (log(double((zn.x - zN.x) * (zn.x - zN.x) + (zn.y - zN.y) * (zn.y - zN.y))) -
-                                 log(double((zo.x - zN.x) * (zo.x - zN.x) + (zo.y - zN.y) * (zo.y - zN.y))));
+        // ln|z' - z_0| - ln|z - z_0| and the same for z_N, in FP32 like the
+        // Jastrow chains
+        const float c02 = __log2f(fmaf(zn.x - z0.x, zn.x - z0.x, (zn.y - z0.y) * (zn.y - z0.y))) -
+                          __log2f(fmaf(zo.x - z0.x, zo.x - z0.x, (zo.y - z0.y) * (zo.y - z0.y)));
+        const float cN2 = __log2f(fmaf(zn.x - zN.x, zn.x - zN.x, (zn.y - zN.y) * (zn.y - zN.y))) -
+                          __log2f(fmaf(zo.x - zN.x, zo.x - zN.x, (zo.y - zN.y) * (zo.y - zN.y)));
+        const double c0 = 0.5 * 0.6931471805599453 * double(c02);
+        const double cN = 0.5 * 0.6931471805599453 * double(cN2);
         delta = mm * (c0 + cN) + guide_delta(gL, zo, zn, a.invR, pl) +
                 guide_delta(gR, zo, zn, a.invR, pr) + 2.0 * mm * lj + 0.5 * gz;
       }
