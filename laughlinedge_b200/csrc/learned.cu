@@ -130,17 +130,20 @@ __device__ NetOut net_eval(const float* __restrict__ P, const float2* zs, int N,
   static_assert(kSlots == 8, "sort8 network");
   static_assert(kNbr <= 32, "one neighbour per lane");
   sort8(key);
+  // every other particle has a finite key, so exactly min(16, N - 1) rounds
+  // pop a neighbour; the rounds are unrolled under that uniform bound
+  const int cnt = min(kNbr, N - 1);
   uint32_t mine = 0xFFFFFFFFu;
-  int cnt = 0;
-  for (int n = 0; n < kNbr; ++n) {
-    const uint32_t m = __reduce_min_sync(0xffffffffu, key[0]);
-    if (m == 0xFFFFFFFFu) break;
-    const bool pop = key[0] == m;  // keys are unique: exactly one lane pops
 #pragma unroll
-    for (int t = 0; t < kSlots - 1; ++t) key[t] = pop ? key[t + 1] : key[t];
-    key[kSlots - 1] = pop ? 0xFFFFFFFFu : key[kSlots - 1];
-    mine = lane == n ? m : mine;
-    ++cnt;
+  for (int n = 0; n < kNbr; ++n) {
+    if (n < cnt) {
+      const uint32_t m = __reduce_min_sync(0xffffffffu, key[0]);
+      const bool pop = key[0] == m;  // keys are unique: exactly one lane pops
+#pragma unroll
+      for (int t = 0; t < kSlots - 1; ++t) key[t] = pop ? key[t + 1] : key[t];
+      key[kSlots - 1] = pop ? 0xFFFFFFFFu : key[kSlots - 1];
+      mine = lane == n ? m : mine;
+    }
   }
   // each lane forms the frame coordinates of its own neighbour once; phi then
   // runs over the neighbours in the same ascending order, their coordinates
@@ -156,10 +159,13 @@ __device__ NetOut net_eval(const float* __restrict__ P, const float2* zs, int N,
   const float2 W0Y = make_float2(P[kOffW1 + 2 * lane + 1], P[kOffW1 + 2 * (lane + 32) + 1]);
   const float2 B0 = make_float2(P[kOffB1 + lane], P[kOffB1 + lane + 32]);
   float2 g = make_float2(0.f, 0.f);
-  for (int n = 0; n < cnt; ++n) {
-    const float a = __shfl_sync(0xffffffffu, xr, n), b = __shfl_sync(0xffffffffu, xt, n);
-    const float2 h = __ffma2_rn(W0X, make_float2(a, a), __ffma2_rn(W0Y, make_float2(b, b), B0));
-    g = __fadd2_rn(g, make_float2(fmaxf(h.x, 0.f), fmaxf(h.y, 0.f)));
+#pragma unroll
+  for (int n = 0; n < kNbr; ++n) {
+    if (n < cnt) {
+      const float a = __shfl_sync(0xffffffffu, xr, n), b = __shfl_sync(0xffffffffu, xt, n);
+      const float2 h = __ffma2_rn(W0X, make_float2(a, a), __ffma2_rn(W0Y, make_float2(b, b), B0));
+      g = __fadd2_rn(g, make_float2(fmaxf(h.x, 0.f), fmaxf(h.y, 0.f)));
+    }
   }
   if (cnt > 0) {
     const float inv = 1.f / float(cnt);
@@ -238,15 +244,23 @@ __device__ Move propose(const float* __restrict__ P, const float2* zs, int N, in
   const float ur = (br - b.mr) * __expf(-b.lr), ut = (bt - b.mt) * __expf(-b.lt);
   const float log_qb = -0.5f * (ur * ur + ut * ut) - b.lr - b.lt;
   // target ratio: m sum_j ln(|z'-z_j|^2 / |z-z_j|^2) - (|z'|^2 - |z|^2) / 2
+  // FP32 products of four squared distances, one log2 per product: for
+  // distances between 1e-4 and 1e4 a product stays within 1e-32 .. 1e32
   float lj = 0.f;
 #pragma unroll
-  for (int t = 0; t < kSlots; ++t) {
-    const int j = lane + 32 * t;
-    if (j < N && j != i) {
-      const float2 zj = zs[j];
-      const float ax = mv.zn.x - zj.x, ay = mv.zn.y - zj.y, ox = zo.x - zj.x, oy = zo.y - zj.y;
-      lj += __log2f(fmaf(ax, ax, ay * ay)) - __log2f(fmaf(ox, ox, oy * oy));
+  for (int t0 = 0; t0 < kSlots; t0 += 4) {
+    float pn = 1.f, po = 1.f;
+#pragma unroll
+    for (int t = t0; t < t0 + 4; ++t) {
+      const int j = lane + 32 * t;
+      if (j < N && j != i) {
+        const float2 zj = zs[j];
+        const float ax = mv.zn.x - zj.x, ay = mv.zn.y - zj.y, ox = zo.x - zj.x, oy = zo.y - zj.y;
+        pn *= fmaf(ax, ax, ay * ay);
+        po *= fmaf(ox, ox, oy * oy);
+      }
     }
+    lj += __log2f(pn) - __log2f(po);
   }
   lj = warp_sum(lj);
   mv.log_a = m * kLn2 * lj - 0.5f * (rn2 - r2) + log_qb - log_qf;
