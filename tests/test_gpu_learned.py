@@ -71,8 +71,8 @@ def _propose(P, zs, i, eps, m, R):
     return (mr, mt, lr, lt, zn[0], zn[1], la, np.sum((zn - zo) ** 2))
 
 
-def _random_params(lemc, rng, sigma=0.4):
-    prop = lemc.LearnedProposal(20, 3, init_sigma=sigma, seed=5)
+def _random_params(lemc, rng, sigma=0.4, N=20):
+    prop = lemc.LearnedProposal(N, 3, init_sigma=sigma, seed=5)
     p = prop.params.copy()
     # make mu and s depend on the neighbourhood
     n_w3 = 4 * H + 4
@@ -92,14 +92,44 @@ def test_network_and_ratio_match_numpy(lemc, cuda_ctx):
     xy = np.stack([rad * np.cos(th), rad * np.sin(th)], -1).astype(np.float32)
     part = rng.integers(0, N, n).astype(np.int32)
     eps = rng.standard_normal((n, 2)).astype(np.float32)
+    _check_against_numpy(prop, xy, part, eps, m, R)
+    prop.close()
+
+
+def _check_against_numpy(prop, xy, part, eps, m, R):
     out = prop.evaluate(xy, part, eps)
     P = _split(prop.params)
-    for s in range(n):
+    for s in range(xy.shape[0]):
         ref = _propose(P, xy[s].astype(np.float64), int(part[s]), eps[s].astype(np.float64), m, R)
         np.testing.assert_allclose(out[s, :4], ref[:4], atol=2e-4, rtol=1e-3)
         np.testing.assert_allclose(out[s, 4:6], ref[4:6], atol=2e-4, rtol=1e-4)
         assert abs(out[s, 6] - ref[6]) < 2e-3 * max(1.0, abs(ref[6])), (s, out[s, 6], ref[6])
         np.testing.assert_allclose(out[s, 7], ref[7], rtol=1e-3, atol=1e-5)
+
+
+def test_neighbour_selection_paths_match_numpy(lemc, cuda_ctx):
+    """N=200 (eight particles per lane, sixteen selection rounds): the
+    network and the ratio against numpy for sampled Laughlin configurations,
+    uniform-disk ones, a tight cluster and a sparse spread."""
+    rng = np.random.default_rng(21)
+    N, m = 200, 3
+    R = math.sqrt(2 * m * N)
+    prop = _random_params(lemc, rng, sigma=1.0, N=N)
+    smp = lemc.Sampler(lemc.SamplerConfig(N, m, 64, step_sigma=1.2, seed=4), [0])
+    smp.init_walkers()
+    smp.run(300, measure=False)
+    laughlin = smp.positions().reshape(64, N, 2)[:12].astype(np.float32)
+    smp.close()
+    n = 12
+    fams = [laughlin]
+    for scale in (1.0, 0.05, 3.0):  # uniform disk, cluster, spread
+        rad = scale * R * np.sqrt(rng.random((n, N)))
+        th = 2 * math.pi * rng.random((n, N))
+        fams.append(np.stack([rad * np.cos(th), rad * np.sin(th)], -1).astype(np.float32))
+    for xy in fams:
+        part = rng.integers(0, N, xy.shape[0]).astype(np.int32)
+        eps = rng.standard_normal((xy.shape[0], 2)).astype(np.float32)
+        _check_against_numpy(prop, np.ascontiguousarray(xy), part, eps, m, R)
     prop.close()
 
 
