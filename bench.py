@@ -50,7 +50,7 @@ WORKLOAD = {
     "particles": 200, "inverse_filling": 3, "omega": 1e-3, "kappa": 5e-6,
     "sectors": list(range(1, 21)), "walkers": 65536, "sigma": 0.3, "seed": 42,
     "gram_mode": "tf32x3", "train_configs": 1 << 20, "train_steps": 5000, "train_batch": 1024,
-    "train_pairs": 32, "tau_walkers": 8192, "tau_sweeps_plain": 6000, "tau_sweeps_learned": 3000,
+    "train_pairs": 32, "tau_walkers": 8192, "tau_sweeps_plain": 12000, "tau_sweeps_learned": 8000,
     "burn": 1000,
 }
 MIXED = {
@@ -338,24 +338,25 @@ def kernel_profile(L, cfg, sectors, steps, proposal=None, init_xy=None, burn=0):
     return st.ms_sweep / steps, st.ms_basis / steps, st.ms_gram / steps
 
 
-def learned_move_flop(N, k_nn=16, hidden=64):
-    """Algorithmic FP32 FLOP of one learned move: two network evaluations
-    (forward at z, reverse at z') of phi (k_nn x 2 -> hidden), rho (hidden+1 ->
-    hidden) and the head (hidden -> 4), 2 FLOP per multiply-add; the two kNN
-    distance scans (3 FLOP per other particle each) and the Jastrow ratio (12
-    FLOP per pair term)."""
+def learned_move_flop(N, reverse=1.0, k_nn=16, hidden=64):
+    """Algorithmic FP32 FLOP of one learned move: the network evaluation at z
+    (phi: k_nn x 2 -> hidden, rho: hidden+1 -> hidden, head: hidden -> 4; 2
+    FLOP per multiply-add) with its kNN distance scan (3 FLOP per other
+    particle), the Jastrow ratio (12 FLOP per pair term), and, for the share
+    `reverse` of moves whose reverse density can change the decision, the
+    second evaluation and scan at z'."""
     net = 2 * (k_nn * 2 * hidden + (hidden + 1) * hidden + hidden * 4)
-    return 2 * net + 2 * 3 * (N - 1) + 12 * (N - 1)
+    return (1.0 + reverse) * (net + 3 * (N - 1)) + 12 * (N - 1)
 
 
-def rooflines(L, w, mode, t_sweep, t_basis, t_gram, learned, clocks):
+def rooflines(L, w, mode, t_sweep, t_basis, t_gram, learned, clocks, reverse=1.0):
     peaks, peak_kind = measured_peaks()
     N, W = w["particles"], w["walkers"]
     sd2, D = sum_d2(w["sectors"], N)
     K = max(4, max(w["sectors"]))
     fp32_peak = 148 * 128 * 2 * peaks.get("sm_max_mhz", 1965.0) / 1e6  # TFLOP/s, nominal at max clock
     if learned:
-        flop_sweep = W * N * learned_move_flop(N)
+        flop_sweep = W * N * learned_move_flop(N, reverse)
     else:
         flop_sweep = W * (12.0 * N * (N - 1) + N * (16.0 * K + 40.0))
     bytes_basis = W * (8.0 * D + 8.0 * K)
@@ -481,7 +482,8 @@ def run_ours(args, ws, rank, local):
     npro = 5
     ks_l = kernel_profile(L, full(w["sigma"]), sectors, npro, proposal=prop, init_xy=start_xy)
     ks_p = kernel_profile(L, full(w["sigma"]), sectors, npro, init_xy=start_xy)
-    roofs = rooflines(L, w, mode, *ks_l, True, clocks)
+    roofs = rooflines(L, w, mode, *ks_l, True, clocks, reverse=st_l.reverse_fraction)
+    roofs["sweep"]["reverse_fraction"] = st_l.reverse_fraction
     roofs_plain = rooflines(L, w, mode, *ks_p, False, clocks)
     dominant = max(roofs, key=lambda k: roofs[k]["ms_per_launch"])
     # the mixed-precision workload's rooflines (N = 50, dL = 0..12), plain sampler

@@ -101,6 +101,9 @@ typedef struct lemc_stats {
   double ms_sweep;          /* device time of the sweep kernels (ms, total)   */
   double ms_basis;          /* device time of the basis build (ms, total)     */
   double ms_gram;           /* device time of the S/H contraction (ms, total) */
+  double reverse_fraction;  /* learned proposal: share of proposed moves whose reverse
+                               density was evaluated (the others could not be accepted
+                               whatever it is); 0 for the Gaussian step                */
 } lemc_stats;
 
 /* One row of the basis returned by lemc_partitions(): the compressed partition

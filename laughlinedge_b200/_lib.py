@@ -47,7 +47,8 @@ class Stats(C.Structure):
     _fields_ = [("sweeps", C.c_uint64), ("measurements", C.c_uint64),
                 ("acceptance", C.c_double), ("tau_int", C.c_double),
                 ("tau_int_each", C.c_double * 4), ("ms_sweep", C.c_double),
-                ("ms_basis", C.c_double), ("ms_gram", C.c_double)]
+                ("ms_basis", C.c_double), ("ms_gram", C.c_double),
+                ("reverse_fraction", C.c_double)]
 
 
 class OccConfig(C.Structure):

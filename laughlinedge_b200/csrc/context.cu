@@ -447,6 +447,7 @@ SweepArgs sweep_args(const lemc_ctx* c, int n_sweeps, int measure) {
   a.rec_p = c->rec_p.p;
   a.rec_w = c->rec_w.p;
   a.accepted = c->accepted.p;
+  a.reverse_evals = c->accepted.p + c->W;
   a.walker_row = c->d_walker_row.p;
   a.guide_pairs = c->d_guide_pairs.p;
   a.guide_npairs = c->d_guide_npairs.p;
@@ -675,9 +676,9 @@ int lemc_create(const lemc_config* cfg, lemc_ctx** out) {
   for (auto& e : c->ev)
     if (st == LEMC_OK && cudaEventCreate(&e) != cudaSuccess) st = LEMC_ERR_CUDA;
   if (st == LEMC_OK) st = c->pos.alloc(size_t(c->W) * c->N);
-  if (st == LEMC_OK) st = c->accepted.alloc(c->W);
+  if (st == LEMC_OK) st = c->accepted.alloc(2 * size_t(c->W));  // accepted | reverse evaluations
   if (st == LEMC_OK) st = c->err.alloc(1);
-  if (st == LEMC_OK && cudaMemset(c->accepted.p, 0, 4 * c->W) != cudaSuccess) st = LEMC_ERR_CUDA;
+  if (st == LEMC_OK && cudaMemset(c->accepted.p, 0, 8 * c->W) != cudaSuccess) st = LEMC_ERR_CUDA;
   if (st == LEMC_OK && cudaMemset(c->err.p, 0, sizeof(int)) != cudaSuccess) st = LEMC_ERR_CUDA;
   if (st != LEMC_OK) {
     lemc_destroy(c);
@@ -829,7 +830,7 @@ static int autotune_lanes(lemc_ctx* c) {
   }
   c->G = bestG;
   ++c->version;
-  if (c->accepted.p) LEMC_CUDA(cudaMemsetAsync(c->accepted.p, 0, 4 * c->W, c->stream));
+  if (c->accepted.p) LEMC_CUDA(cudaMemsetAsync(c->accepted.p, 0, 8 * c->W, c->stream));
   LEMC_CUDA(cudaStreamSynchronize(c->stream));
   save.release();
   return LEMC_OK;
@@ -869,7 +870,7 @@ int lemc_reset_accumulators(lemc_ctx* c) {
   if (c->rowacc.p) LEMC_CUDA(cudaMemsetAsync(c->rowacc.p, 0, sizeof(double) * c->rowacc.n, c->stream));
   if (c->tc_partials.p)
     LEMC_CUDA(cudaMemsetAsync(c->tc_partials.p, 0, sizeof(double) * c->tc_partials.n, c->stream));
-  if (c->accepted.p) LEMC_CUDA(cudaMemsetAsync(c->accepted.p, 0, 4 * c->W, c->stream));
+  if (c->accepted.p) LEMC_CUDA(cudaMemsetAsync(c->accepted.p, 0, 8 * c->W, c->stream));
   if (c->err.p) LEMC_CUDA(cudaMemsetAsync(c->err.p, 0, sizeof(int), c->stream));
   c->meas = 0;
   c->bins.clear();
@@ -1118,7 +1119,7 @@ static int autotune_gram_splits(lemc_ctx* c) {
   LEMC_TRY(setup_tc(c, best_sp));
   LEMC_CUDA(cudaMemcpyAsync(c->pos.p, save.p, sizeof(float2) * c->W * c->N,
                             cudaMemcpyDeviceToDevice, c->stream));
-  if (c->accepted.p) LEMC_CUDA(cudaMemsetAsync(c->accepted.p, 0, 4 * c->W, c->stream));
+  if (c->accepted.p) LEMC_CUDA(cudaMemsetAsync(c->accepted.p, 0, 8 * c->W, c->stream));
   LEMC_CUDA(cudaMemsetAsync(c->tc_partials.p, 0, sizeof(double) * c->tc_partials.n, c->stream));
   LEMC_CUDA(cudaMemsetAsync(c->gram.p, 0, sizeof(double) * c->gram.n, c->stream));
   LEMC_CUDA(cudaStreamSynchronize(c->stream));
@@ -1327,15 +1328,20 @@ int lemc_read_rows(lemc_ctx* c, double omega, double kappa, double* fg, double* 
 int lemc_read_stats(lemc_ctx* c, lemc_stats* st) {
   if (!c || !st) return LEMC_ERR_ARG;
   std::memset(st, 0, sizeof(*st));
-  std::vector<uint32_t> acc(c->W);
-  LEMC_CUDA(cudaMemcpyAsync(acc.data(), c->accepted.p, 4 * c->W, cudaMemcpyDeviceToHost, c->stream));
+  std::vector<uint32_t> acc(2 * size_t(c->W));
+  LEMC_CUDA(cudaMemcpyAsync(acc.data(), c->accepted.p, 8 * c->W, cudaMemcpyDeviceToHost, c->stream));
   LEMC_TRY(lemc_synchronize(c));
-  double tot = 0;
-  for (uint32_t a : acc) tot += a;
+  double tot = 0, rev = 0;
+  for (int w = 0; w < c->W; ++w) {
+    tot += acc[w];
+    rev += acc[c->W + w];
+  }
   const double swept = double(c->sweeps - c->sweeps_at_reset);
+  const double moves = swept * c->W * c->N;
   st->sweeps = c->sweeps;
   st->measurements = c->meas;
-  st->acceptance = swept > 0 ? tot / (swept * c->W * c->N) : 0.0;
+  st->acceptance = swept > 0 ? tot / moves : 0.0;
+  st->reverse_fraction = swept > 0 ? rev / moves : 0.0;
   // tau_int: Sokal windowing on the walker-mean series of Re and Im p_k; NaN
   // (for that k, and then for the maximum) when the series is too short for a
   // self-consistent window.

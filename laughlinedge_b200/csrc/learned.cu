@@ -12,6 +12,10 @@
 // where q(z | z') is the same network evaluated at the proposed configuration
 // (its own neighbours and frame), so the chain samples |Psi_m|^2 exactly
 // whatever the weights are.  Weights are stored in BF16, arithmetic is FP32.
+// Since ln s >= ln(1/4), ln q(z | z') <= 2 ln 4: a sweep evaluates the reverse
+// network only when ln u < ln A_forward + 2 ln 4 (ln A_forward: everything but
+// the reverse density), which skips it for moves that would be rejected
+// whatever its value, with the same decisions as the full ratio.
 //
 // Sampler layout: one walker per warp, positions in shared memory, lane l
 // owns particles l, l+32, ...  The 16 neighbours are found from packed
@@ -54,7 +58,9 @@ constexpr int kOffW3 = kOffB2 + kH;        // [4][kH]
 constexpr int kOffB3 = kOffW3 + 4 * kH;    // [4]
 constexpr int kNParams = kOffB3 + 4;
 constexpr float kInScale = 0.5f;           // displacement feature scale (1 / 2 l_B)
-constexpr float kLogSMin = -3.912023f;     // log 0.02
+// proposal scales s in [1/4, 4] (units of l_B): the lower bound also bounds
+// the reverse density, which lets a sweep skip it for hopeless moves
+constexpr float kLogSMin = -1.386294f;     // log 1/4
 constexpr float kLogSMax = 1.386294f;      // log 4
 constexpr int kMaxN = 256;                 // packed kNN keys carry 8 index bits
 constexpr int kSlots = kMaxN / 32;         // particles per lane
@@ -214,8 +220,23 @@ struct Move {
   float jump2;     // |z' - z|^2
 };
 
-__device__ Move propose(const float* __restrict__ P, const float2* zs, int N, int i, float invR,
-                        float m, float e_r, float e_t, int lane, float* gbuf) {
+// The forward half of a move: the network at z_i, the proposed position, and
+// part = ln|Psi(z')|^2 - ln|Psi(z)|^2 - ln q(z' | z), so that
+// ln A = part + ln q(z | z') (reverse_log_density) in FP32 as written.
+struct Forward {
+  float2 zn;
+  float part;
+  float jump2;
+};
+
+// ln q(z | z') = -|u|^2 / 2 - ln s_r' - ln s_t' <= -2 kLogSMin, because
+// ln s >= kLogSMin after the clamp and every FP32 rounding is monotone; hence
+// ln A = part + ln q(z | z') never exceeds part + kLogQbMax in FP32 either.
+constexpr float kLogQbMax = -2.f * kLogSMin;
+
+__device__ Forward propose_forward(const float* __restrict__ P, const float2* zs, int N, int i,
+                                   float invR, float m, float e_r, float e_t, int lane,
+                                   float* gbuf) {
   const float2 zo = zs[i];
   const NetOut f = net_eval(P, zs, N, i, zo, invR, lane, gbuf);
   const float sr = __expf(f.lr), st = __expf(f.lt);
@@ -227,22 +248,9 @@ __device__ Move propose(const float* __restrict__ P, const float2* zs, int N, in
     c = zo.x * ri;
     s = zo.y * ri;
   }
-  Move mv;
-  mv.zn = make_float2(zo.x + (c * dr - s * dt), zo.y + (s * dr + c * dt));
+  Forward fw;
+  fw.zn = make_float2(zo.x + (c * dr - s * dt), zo.y + (s * dr + c * dt));
   const float log_qf = -0.5f * (e_r * e_r + e_t * e_t) - f.lr - f.lt;
-  // reverse proposal: the network at the proposed configuration
-  const NetOut b = net_eval(P, zs, N, i, mv.zn, invR, lane, gbuf);
-  const float rn2 = mv.zn.x * mv.zn.x + mv.zn.y * mv.zn.y;
-  float cb = 1.f, sb = 0.f;
-  if (rn2 > 1e-20f) {
-    const float ri = rsqrtf(rn2);
-    cb = mv.zn.x * ri;
-    sb = mv.zn.y * ri;
-  }
-  const float bx = zo.x - mv.zn.x, by = zo.y - mv.zn.y;
-  const float br = bx * cb + by * sb, bt = by * cb - bx * sb;
-  const float ur = (br - b.mr) * __expf(-b.lr), ut = (bt - b.mt) * __expf(-b.lt);
-  const float log_qb = -0.5f * (ur * ur + ut * ut) - b.lr - b.lt;
   // target ratio: m sum_j ln(|z'-z_j|^2 / |z-z_j|^2) - (|z'|^2 - |z|^2) / 2
   // FP32 products of four squared distances, one log2 per product: for
   // distances between 1e-4 and 1e4 a product stays within 1e-32 .. 1e32
@@ -255,7 +263,7 @@ __device__ Move propose(const float* __restrict__ P, const float2* zs, int N, in
       const int j = lane + 32 * t;
       if (j < N && j != i) {
         const float2 zj = zs[j];
-        const float ax = mv.zn.x - zj.x, ay = mv.zn.y - zj.y, ox = zo.x - zj.x, oy = zo.y - zj.y;
+        const float ax = fw.zn.x - zj.x, ay = fw.zn.y - zj.y, ox = zo.x - zj.x, oy = zo.y - zj.y;
         pn *= fmaf(ax, ax, ay * ay);
         po *= fmaf(ox, ox, oy * oy);
       }
@@ -263,8 +271,38 @@ __device__ Move propose(const float* __restrict__ P, const float2* zs, int N, in
     lj += __log2f(pn) - __log2f(po);
   }
   lj = warp_sum(lj);
-  mv.log_a = m * kLn2 * lj - 0.5f * (rn2 - r2) + log_qb - log_qf;
-  mv.jump2 = fmaf(c * dr - s * dt, c * dr - s * dt, (s * dr + c * dt) * (s * dr + c * dt));
+  const float rn2 = fw.zn.x * fw.zn.x + fw.zn.y * fw.zn.y;
+  const float dlp = m * kLn2 * lj - 0.5f * (rn2 - r2);
+  fw.part = dlp - log_qf;
+  fw.jump2 = fmaf(c * dr - s * dt, c * dr - s * dt, (s * dr + c * dt) * (s * dr + c * dt));
+  return fw;
+}
+
+// ln q(z_i | z'): the network at the proposed configuration (particle i at zn).
+__device__ float reverse_log_density(const float* __restrict__ P, const float2* zs, int N, int i,
+                                     float2 zn, float invR, int lane, float* gbuf) {
+  const float2 zo = zs[i];
+  const NetOut b = net_eval(P, zs, N, i, zn, invR, lane, gbuf);
+  const float rn2 = zn.x * zn.x + zn.y * zn.y;
+  float cb = 1.f, sb = 0.f;
+  if (rn2 > 1e-20f) {
+    const float ri = rsqrtf(rn2);
+    cb = zn.x * ri;
+    sb = zn.y * ri;
+  }
+  const float bx = zo.x - zn.x, by = zo.y - zn.y;
+  const float br = bx * cb + by * sb, bt = by * cb - bx * sb;
+  const float ur = (br - b.mr) * __expf(-b.lr), ut = (bt - b.mt) * __expf(-b.lt);
+  return -0.5f * (ur * ur + ut * ut) - b.lr - b.lt;
+}
+
+__device__ Move propose(const float* __restrict__ P, const float2* zs, int N, int i, float invR,
+                        float m, float e_r, float e_t, int lane, float* gbuf) {
+  const Forward fw = propose_forward(P, zs, N, i, invR, m, e_r, e_t, lane, gbuf);
+  Move mv;
+  mv.zn = fw.zn;
+  mv.log_a = fw.part + reverse_log_density(P, zs, N, i, fw.zn, invR, lane, gbuf);
+  mv.jump2 = fw.jump2;
   return mv;
 }
 
@@ -298,7 +336,7 @@ learned_sweep_kernel(const SweepArgs a, const __nv_bfloat16* __restrict__ wts) {
   __syncwarp();
   const uint32_t sweep_base = a.sweep0 + (a.sweep_ctr ? *a.sweep_ctr : 0u);
   const float m = float(a.m);
-  uint32_t nacc = 0;
+  uint32_t nacc = 0, nrev = 0;
   for (int sw = 0; sw < a.n_sweeps; ++sw) {
     const uint32_t sweep = sweep_base + uint32_t(sw);
     float er_l = 0.f, et_l = 0.f, lu_l = 0.f;
@@ -314,11 +352,18 @@ learned_sweep_kernel(const SweepArgs a, const __nv_bfloat16* __restrict__ wts) {
       const float er = __shfl_sync(0xffffffffu, er_l, i & 31);
       const float et = __shfl_sync(0xffffffffu, et_l, i & 31);
       const float lu = __shfl_sync(0xffffffffu, lu_l, i & 31);
-      const Move mv = propose(P, zs, N, i, a.invR, m, er, et, lane, gsm[wib]);
-      const bool acc = lu < mv.log_a;
+      // the reverse density is only evaluated when it can change the decision:
+      // if ln u >= part + kLogQbMax, ln u >= ln A in FP32 and the move is
+      // rejected as the full ratio would reject it (warp-uniform test)
+      const Forward fw = propose_forward(P, zs, N, i, a.invR, m, er, et, lane, gsm[wib]);
+      bool acc = false;
+      if (lu < fw.part + kLogQbMax) {
+        acc = lu < fw.part + reverse_log_density(P, zs, N, i, fw.zn, a.invR, lane, gsm[wib]);
+        ++nrev;
+      }
       __syncwarp();
       if (acc) {
-        if (lane == (i & 31)) zs[i] = mv.zn;
+        if (lane == (i & 31)) zs[i] = fw.zn;
         ++nacc;
       }
       __syncwarp();
@@ -326,6 +371,7 @@ learned_sweep_kernel(const SweepArgs a, const __nv_bfloat16* __restrict__ wts) {
   }
   for (int j = lane; j < N; j += 32) a.pos[size_t(w) * N + j] = zs[j];
   if (a.accepted && lane == 0) a.accepted[w] += nacc;
+  if (a.reverse_evals && lane == 0) a.reverse_evals[w] += nrev;
   if (!a.measure) return;
   // measurement record, the plain sweep's layout: four degrees per pass over
   // the particles (w^k by the same sequence of multiplications in every pass),

@@ -17,6 +17,7 @@ struct SweepArgs {
   float2* rec_p;            // [K][W] power sums p_1..p_K (measure != 0)
   float* rec_w;             // [LEMC_N_WEIGHTS][W] weight planes (measure != 0)
   uint32_t* accepted;       // [W] accumulated accepted moves (may be null)
+  uint32_t* reverse_evals;  // [W] moves whose reverse density was evaluated (learned; may be null)
   const int32_t* walker_row;   // [W] guide row (row guide only)
   const int32_t* guide_pairs;  // [rows][2*kMaxGuideParts] (part, mult)
   const int32_t* guide_npairs; // [rows]

@@ -47,7 +47,7 @@ def _net(P, zs, i, zc, R):
     g /= len(sel)
     k = np.maximum(W2[:, :H] @ g + W2[:, H] * (r / R - 1.0) + b2, 0.0)
     o = W3 @ k + b3
-    return o[0], o[1], np.clip(o[2], math.log(0.02), math.log(4.0)), np.clip(o[3], math.log(0.02), math.log(4.0))
+    return o[0], o[1], np.clip(o[2], math.log(0.25), math.log(4.0)), np.clip(o[3], math.log(0.25), math.log(4.0))
 
 
 def _propose(P, zs, i, eps, m, R):
@@ -141,9 +141,14 @@ def _r2_mean(lemc, N, m, W, seed, proposal=None):
     smp.run(600, measure=False)
     smp.run(200, measure=True)
     S, H2, _, _ = smp.gram(0)
-    acc = smp.stats().acceptance
+    st = smp.stats()
     smp.close()
-    return float(np.real(H2[0, 0] / S[0, 0])), acc
+    # every accepted move had its reverse density evaluated; the Gaussian step has none
+    if proposal is None:
+        assert st.reverse_fraction == 0.0
+    else:
+        assert st.acceptance <= st.reverse_fraction <= 1.0, (st.acceptance, st.reverse_fraction)
+    return float(np.real(H2[0, 0] / S[0, 0])), st.acceptance
 
 
 def test_learned_sampler_is_exact(lemc, cuda_ctx):
