@@ -9,9 +9,11 @@ block back.  Launch order on the context stream: the walker initialisation,
 one contraction (plus the per-sector reduce at the end), so ``-s``/``-c`` of a
 profiler select e.g. the third contraction with ``-k regex:gram_tc -s 2 -c 1``.
 
-``python tests/profile_case.py learned [walkers]`` builds the DeepSets proposal
-(N=200, m=3, init sigma 0.3, seed 5, untrained weights) and a W-walker context
-(default 4096) that uses it, and runs three single unmeasured sweeps.
+``python tests/profile_case.py learned [walkers]`` burns in a W-walker plain
+context (N=200, m=3, default W=4096, 300 sweeps), trains the DeepSets
+proposal on its configurations (init sigma 1.24, 1000 ES steps), then runs
+three single unmeasured learned sweeps from the burnt-in walkers; the learned
+sweeps are the last three launches of `learned_sweep_kernel`.
 
 ``python tests/profile_case.py occupation [walkers] [sweeps]`` runs one
 occupation estimate (N=50, m=3, dL=4, l_cutoff = m(N-1)+15, sweeps/2 burn-in
@@ -29,15 +31,27 @@ from laughlinedge_b200.sampler import occupation  # noqa: E402
 
 
 def learned(argv) -> int:
+    import torch
     W = int(argv[0]) if argv else 4096
-    prop = LearnedProposal(200, 3, init_sigma=0.3, seed=5)
-    smp = Sampler(SamplerConfig(200, 3, W, step_sigma=0.3, seed=1), [1])
+    N, m = 200, 3
+    burn = Sampler(SamplerConfig(N, m, W, step_sigma=1.24, seed=1), [1])
+    burn.init_walkers()
+    burn.run(300, measure=False)
+    cfg = torch.empty((W, N, 2), dtype=torch.float32, device="cuda")
+    burn.copy_positions_device(cfg.data_ptr())
+    burn.synchronize()
+    xy = burn.positions()
+    burn.close()
+    prop = LearnedProposal(N, m, init_sigma=1.24, seed=5)
+    prop.train(cfg.data_ptr(), W, steps=1000, batch=1024, pairs=32, lr=3e-3)
+    smp = Sampler(SamplerConfig(N, m, W, step_sigma=0.3, seed=1, lanes_per_walker=0), [1])
     smp.set_proposal(prop)
-    smp.init_walkers()
+    smp.init_walkers(xy)
     for _ in range(3):
         smp.run(1, measure=False)
     smp.synchronize()
-    print("ok", smp.stats().acceptance)
+    st = smp.stats()
+    print("ok", st.acceptance, st.reverse_fraction)
     smp.close()
     prop.close()
     return 0
