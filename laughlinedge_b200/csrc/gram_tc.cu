@@ -9,16 +9,18 @@
 //
 // Precision: each FP32 operand x is split x = hi + lo with hi = bf16(x),
 // lo = bf16(x - hi) (kind::f16) or hi = tf32_rn(x), lo = tf32_rn(x - hi)
-// (kind::tf32).  hi*hi accumulates in one FP32 tensor-memory accumulator and
-// the correction products hi*lo + lo*hi (+ lo*lo) in a second one.  The
-// tensor core's accumulation truncates (a relative bias of about -4e-8 per
-// MMA step), so every `flush_every` K-chunks the epilogue warps move the hi*hi
-// accumulator out of tensor memory into FP32 register sums (round-to-nearest;
-// two hi*hi buffers let the MMAs continue meanwhile).  The correction
-// accumulator is 2^-11 (TF32) or 2^-8 (BF16) of the result, so its own bias
-// stays far below the target and it is read once, after the last K-chunk.  At
-// the end each job adds its sums, in FP64, to its private slot in global
-// memory.
+// (kind::tf32).  Each accumulator buffer holds 192 FP32 columns: hi*hi in the
+// first 96 and the correction products hi*lo + lo*hi (+ lo*lo) in the next 96.
+// One M=128 x N=192 MMA multiplies A_hi by the stacked [B_hi; B_lo] operand
+// (both products at once) and one N=96 MMA adds A_lo * B_hi to the
+// corrections.  A tcgen05.mma of kind::tf32 with K=8 costs about 97 cycles for
+// any N up to 128 and 106 cycles at N=192 (measured on B200), so this takes
+// 203 cycles per K step where three N=96 MMAs took 290.  The tensor core's
+// accumulation truncates (a relative bias of about -4e-8 per MMA step), so
+// every `flush_every` K-chunks the epilogue warps move both halves of the
+// buffer out of tensor memory into FP32 register sums (round-to-nearest; two
+// buffers let the MMAs continue meanwhile).  At the end each job adds its
+// sums, in FP64, to its private slot in global memory.
 //
 // Operand placement.  The A operand (hi and lo, 128 rows x one K-chunk) lives
 // in tensor memory: the A converters write it with tcgen05.st and the MMAs
@@ -42,8 +44,8 @@
 // workload.)
 //   warps 0-7    epilogue: TMEM lane quarter = warp % 4, column half =
 //                warp / 4, 48 FP32 accumulators per thread.
-// Tensor memory columns: hi*hi buffers at 0 and 128, corrections at 256, A
-// stages at 384 and 448 (hi at +0, lo at +32).
+// Tensor memory columns: accumulator buffers at 0 and 192 (hi*hi at +0,
+// corrections at +96), A stages at 384 and 448 (hi at +0, lo at +32).
 // No load uses cluster multicast; every source is this GPU's own memory.
 // Every mbarrier wait is bounded in time; on expiry the kernel records
 // LEMC_ERR_TIMEOUT in the error word, skips its output and unwinds: the loader
@@ -76,9 +78,10 @@ constexpr int kLoadWarp = 17;
 constexpr int kSchedWarp = 18;     // does the issuer's barrier waits (see the MMA issuer)
 constexpr int kThreads = 19 * 32;
 constexpr int kTmemCols = 512;
-constexpr uint32_t kColHH = 0;     // hi*hi buffers at 0 and 128
-constexpr uint32_t kColCorr = 256; // corrections
+constexpr uint32_t kColBuf = 0;    // accumulator buffers at 0 and 192 (hi*hi +0, corrections +96)
+constexpr uint32_t kBufCols = 2 * kN;
 constexpr uint32_t kColA = 384;    // A stages at 384 + 64 s (hi +0, lo +32)
+static_assert(2 * kBufCols <= kColA, "accumulator buffers overlap the A stages");
 constexpr long long kWaitCycles = 4000000000LL;  // default wait bound, ~2 s at 1.9 GHz
 
 template <bool TF32>
@@ -103,7 +106,6 @@ struct Smem {
   uint64_t op_empty[kOpStages];
   uint64_t acc_full[2];
   uint64_t acc_empty[2];
-  uint64_t corr_full;
   uint64_t done;
   uint32_t tmem_base;
   int abort_flag;
@@ -203,9 +205,9 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
   return d;
 }
 
-// Instruction descriptor: dense, FP32 accumulate, A/B K-major, M=128, N=96.
-__host__ __device__ constexpr uint32_t make_idesc(uint32_t ab_format) {
-  return (1u << 4) | (ab_format << 7) | (ab_format << 10) | (uint32_t(kN >> 3) << 17) |
+// Instruction descriptor: dense, FP32 accumulate, A/B K-major, M=128, N=n.
+__host__ __device__ constexpr uint32_t make_idesc(uint32_t ab_format, int n) {
+  return (1u << 4) | (ab_format << 7) | (ab_format << 10) | (uint32_t(n >> 3) << 17) |
          (uint32_t(kM >> 4) << 24);
 }
 
@@ -335,7 +337,8 @@ gram_tc_kernel(const TcArgs a, const __grid_constant__ CUtensorMap tmA,
   constexpr int KC = C::KC;
   constexpr int EPC = TF32 ? 4 : 8;          // elements per 16-byte B operand chunk
   constexpr int NKSTEP = kOpRowBytes / 32;   // one MMA consumes 32 bytes of K
-  constexpr uint32_t IDESC = make_idesc(TF32 ? 2u : 1u);
+  constexpr uint32_t IDESC = make_idesc(TF32 ? 2u : 1u, kN);          // N=96
+  constexpr uint32_t IDESC2 = make_idesc(TF32 ? 2u : 1u, 2 * kN);     // N=192: [B_hi; B_lo]
   constexpr int RS = C::RAW_STAGES;
 
   extern __shared__ __align__(1024) uint8_t smem_raw[];
@@ -365,7 +368,6 @@ gram_tc_kernel(const TcArgs a, const __grid_constant__ CUtensorMap tmA,
       mbar_init(&sm->acc_full[b], 1);
       mbar_init(&sm->acc_empty[b], kEpiWarps * 32);
     }
-    mbar_init(&sm->corr_full, 1);
     mbar_init(&sm->done, 1);
     sm->abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -567,24 +569,23 @@ gram_tc_kernel(const TcArgs a, const __grid_constant__ CUtensorMap tmA,
         tc_fence_after();
         const uint64_t bh = s ? bdesc1 : bdesc0, bl = bh + kLoDesc;
         const uint32_t ahi = tmem + kColA + uint32_t(s * 64), alo = ahi + 32;
-        const uint32_t d = tmem + kColHH + uint32_t(b * 128);
-        const uint32_t dc = tmem + kColCorr;
-        const uint32_t acc_d = f == 0 ? 0u : 1u, acc_c = c == 0 ? 0u : 1u;
-        // K step ks: B advances 32 bytes (2 descriptor units), A 8 TMEM columns
-        mma_ts<TF32>(d, ahi, bh, IDESC, acc_d);
-        mma_ts<TF32>(dc, ahi, bl, IDESC, acc_c);
+        const uint32_t d = tmem + kColBuf + uint32_t(b) * kBufCols;  // hi*hi | corrections
+        const uint32_t dc = d + kN;
+        // the first MMA of a flush group overwrites both halves of the buffer
+        const uint32_t acc_d = f == 0 ? 0u : 1u;
+        // K step ks: B advances 32 bytes (2 descriptor units), A 8 TMEM columns;
+        // the B hi and lo tiles are contiguous, so bh with N=192 spans both
+        mma_ts<TF32>(d, ahi, bh, IDESC2, acc_d);
         mma_ts<TF32>(dc, alo, bh, IDESC, 1u);
         if (four) mma_ts<TF32>(dc, alo, bl, IDESC, 1u);
 #pragma unroll
         for (int ks = 1; ks < NKSTEP; ++ks) {
-          mma_ts<TF32>(d, ahi + 8 * ks, bh + 2 * ks, IDESC, 1u);
-          mma_ts<TF32>(dc, ahi + 8 * ks, bl + 2 * ks, IDESC, 1u);
+          mma_ts<TF32>(d, ahi + 8 * ks, bh + 2 * ks, IDESC2, 1u);
           mma_ts<TF32>(dc, alo + 8 * ks, bh + 2 * ks, IDESC, 1u);
           if (four) mma_ts<TF32>(dc, alo + 8 * ks, bl + 2 * ks, IDESC, 1u);
         }
         umma_commit(&sm->op_empty[s]);
         if (f + 1 == F || c == nch - 1) umma_commit(&sm->acc_full[b]);
-        if (c == nch - 1) umma_commit(&sm->corr_full);
         ++issued;
       }
       __syncwarp();
@@ -621,40 +622,27 @@ gram_tc_kernel(const TcArgs a, const __grid_constant__ CUtensorMap tmA,
         break;
       }
       tc_fence_after();
-      const uint32_t ta = tmem + lane_base + kColHH + uint32_t(b * 128 + part0);
+      // hi*hi column j and its correction column j + 96 belong to one sum
+      const uint32_t ta = tmem + lane_base + kColBuf + uint32_t(b) * kBufCols + uint32_t(part0);
 #pragma unroll
-      for (int part = 0; part < kEpiCols / 16; ++part) {
+      for (int part = 0; part < kEpiCols / 8; ++part) {
         uint32_t v0[8], v1[8];
-        tmem_ld8(ta + part * 16, v0);
-        tmem_ld8(ta + part * 16 + 8, v1);
+        tmem_ld8(ta + part * 8, v0);
+        tmem_ld8(ta + kN + part * 8, v1);
         tmem_wait_ld();
-        if (part == kEpiCols / 16 - 1) {
+        if (part == kEpiCols / 8 - 1) {
           // every column of this buffer is in registers: the MMAs may reuse it
           tc_fence_before();
           mbar_arrive(&sm->acc_empty[b]);
         }
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
-          sum[part * 16 + i] += __uint_as_float(v0[i]);
-          sum[part * 16 + 8 + i] += __uint_as_float(v1[i]);
+          sum[part * 8 + i] += __uint_as_float(v0[i]);
+          sum[part * 8 + i] += __uint_as_float(v1[i]);
         }
       }
     }
-    if (ok && nch > 0 && mbar_wait(&sm->corr_full, 0u, abort_flag, a.err, a.wait_cycles)) {
-      tc_fence_after();
-      const uint32_t ta = tmem + lane_base + kColCorr + uint32_t(part0);
-#pragma unroll
-      for (int part = 0; part < kEpiCols / 16; ++part) {
-        uint32_t v0[8], v1[8];
-        tmem_ld8(ta + part * 16, v0);
-        tmem_ld8(ta + part * 16 + 8, v1);
-        tmem_wait_ld();
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-          sum[part * 16 + i] += __uint_as_float(v0[i]);
-          sum[part * 16 + 8 + i] += __uint_as_float(v1[i]);
-        }
-      }
+    if (ok && nch > 0) {
       if (!*(volatile int*)abort_flag) {
         double* slot = a.partials + (size_t)tile.slot * (kM * kN) +
                        (size_t)(quarter * 32 + lane) * kN + part0;
