@@ -327,8 +327,11 @@ LEMC_API int lemc_gram_device(lemc_ctx* ctx, const void* V, const void* rec_w, i
  * (mu_r, mu_t, log s_r, log s_t) of the proposed move z' = z + Rot(theta)(mu
  * + s eps).  A context using it (lemc_set_proposal) accepts with the exact
  * ratio |Psi(z')|^2 q(z|z') / (|Psi(z)|^2 q(z'|z)), so it samples |Psi_m|^2
- * for any weights.  Weights: FP32 master copy, BF16 copy used by the kernels.
- * particles <= 256; Laughlin guide only. */
+ * for any weights.  The scales are clamped to s in [1, 4] (units of l_B); the
+ * lower bound gives ln q(z|z') <= 0, so a sweep skips the reverse network for
+ * moves that ln u already rejects (lemc_stats.reverse_fraction reports the
+ * share it evaluated) with unchanged decisions.  Weights: FP32 master copy,
+ * BF16 copy used by the kernels.  particles <= 256; Laughlin guide only. */
 typedef struct lemc_proposal lemc_proposal;
 typedef struct lemc_train_config {
   int32_t steps;      /* Adam steps */
@@ -341,8 +344,8 @@ typedef struct lemc_train_config {
 /* Number of network parameters (FP32 layout W1[64][2], b1[64], W2[64][65], b2[64],
  * W3[4][64], b3[4]). */
 LEMC_API int lemc_proposal_n_params(int* n);
-/* New proposal initialised to the plain isotropic step init_sigma (hidden
- * weights random from seed, output weights near zero). */
+/* New proposal initialised to the plain isotropic step init_sigma (clamped to
+ * [1, 4]; hidden weights random from seed, output weights near zero). */
 LEMC_API int lemc_proposal_create(int particles, int inverse_filling, float init_sigma,
                                   uint64_t seed, lemc_proposal** out);
 LEMC_API int lemc_proposal_destroy(lemc_proposal* p);
