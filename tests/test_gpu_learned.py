@@ -184,3 +184,59 @@ def test_training_raises_the_objective(lemc, cuda_ctx):
     assert trace[-30:].mean() > 1.05 * trace[:30].mean(), (trace[:30].mean(), trace[-30:].mean())
     smp.close()
     prop.close()
+
+
+def _u01(x):
+    # lemc_rng.h u01: ((x >> 9) + 1/2) * 2^-23, exact in FP32
+    return (float(x >> 9) + 0.5) * 2.0 ** -23
+
+
+def test_learned_chain_matches_numpy_move_by_move(lemc, oracle, cuda_ctx):
+    """Two sweeps of the learned sampler (N=20, 24 walkers) against a numpy
+    restatement that always evaluates the full Metropolis-Hastings ratio with
+    the same Philox draws {move, sweep, walker, 4}: the sweep's early
+    rejection (the reverse network skipped when ln u >= ln A without it)
+    must take the same decisions.  A walker may leave the numpy trajectory
+    only at a near tie |ln A - ln u| < 1e-3 (FP32 network against FP64)."""
+    rng = np.random.default_rng(31)
+    N, m, W, seed, n_sweeps = 20, 3, 24, 977, 2
+    R = math.sqrt(2 * m * N)
+    prop = _random_params(lemc, rng, sigma=1.5, N=N)
+    smp = lemc.Sampler(lemc.SamplerConfig(N, m, W, step_sigma=0.3, seed=seed), [0])
+    smp.set_proposal(prop)
+    rad = R * np.sqrt(rng.random((W, N)))
+    th = 2 * math.pi * rng.random((W, N))
+    xy0 = np.stack([rad * np.cos(th), rad * np.sin(th)], -1).astype(np.float32)
+    smp.init_walkers(xy0)
+    smp.run(n_sweeps, measure=False)
+    got = smp.positions().reshape(W, N, 2)
+    st = smp.stats()
+    smp.close()
+    P = _split(prop.params)
+    key = (seed & 0xFFFFFFFF, seed >> 32)
+    good, ties, skipped = 0, 0, 0
+    for w in range(W):
+        zs = xy0[w].astype(np.float64).copy()
+        margin = np.inf
+        for sw in range(n_sweeps):
+            for i in range(N):
+                r = oracle.philox([i, sw, w, 4], key)
+                rad_ = math.sqrt(-2.0 * math.log(_u01(r[0])))
+                ang = 2.0 * math.pi * _u01(r[1])
+                eps = np.array([rad_ * math.cos(ang), rad_ * math.sin(ang)])
+                lu = math.log(_u01(r[2]))
+                out = _propose(P, zs.astype(np.float32).astype(np.float64), i, eps, m, R)
+                la = out[6]
+                margin = min(margin, abs(la - lu))
+                if lu < la:
+                    zs[i] = [out[4], out[5]]
+        if np.allclose(got[w], zs, atol=2e-3, rtol=0):
+            good += 1
+        else:
+            assert margin < 1e-3, (w, margin)
+            ties += 1
+    assert good >= W - 2, (good, ties)
+    # the early rejection ran: fewer reverse evaluations than moves, and
+    # never fewer than accepted moves
+    assert st.acceptance <= st.reverse_fraction < 1.0, (st.acceptance, st.reverse_fraction)
+    prop.close()
