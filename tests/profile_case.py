@@ -15,6 +15,12 @@ proposal on its configurations (init sigma 1.24, 1000 ES steps), then runs
 three single unmeasured learned sweeps from the burnt-in walkers; the learned
 sweeps are the last three launches of `learned_sweep_kernel`.
 
+``python tests/profile_case.py learned_step [walkers] [steps]`` runs the
+learned workload's full step: N=200, m=3, dL 1..20, TF32x3, default W=65536;
+300 plain burn-in sweeps, a proposal trained for 1000 ES steps on those
+walkers, then 2 unmeasured learned sweeps and `steps` (default 4) measured
+steps (learned sweep -> basis -> contraction).
+
 ``python tests/profile_case.py occupation [walkers] [sweeps]`` runs one
 occupation estimate (N=50, m=3, dL=4, l_cutoff = m(N-1)+15, sweeps/2 burn-in
 + sweeps measured in one launch; defaults 65536 walkers, 100 sweeps).
@@ -57,6 +63,37 @@ def learned(argv) -> int:
     return 0
 
 
+def learned_step(argv) -> int:
+    import torch
+    W = int(argv[0]) if argv else 65536
+    steps = int(argv[1]) if len(argv) > 1 else 4
+    N, m = 200, 3
+    sectors = list(range(1, 21))
+    burn = Sampler(SamplerConfig(N, m, W, step_sigma=1.24, seed=1, lanes_per_walker=8), [1])
+    burn.init_walkers()
+    burn.run(300, measure=False)
+    cfg = torch.empty((W, N, 2), dtype=torch.float32, device="cuda")
+    burn.copy_positions_device(cfg.data_ptr())
+    burn.synchronize()
+    xy = burn.positions()
+    burn.close()
+    prop = LearnedProposal(N, m, init_sigma=1.24, seed=5)
+    prop.train(cfg.data_ptr(), W, steps=1000, batch=1024, pairs=32, lr=3e-3)
+    del cfg
+    smp = Sampler(SamplerConfig(N, m, W, step_sigma=0.3, seed=1, lanes_per_walker=0,
+                                gram_mode=3), sectors)
+    smp.set_proposal(prop)
+    smp.init_walkers(xy)
+    smp.run(2, measure=False)
+    smp.run(steps, measure=True)
+    smp.synchronize()
+    st = smp.stats()
+    print("ok", st.acceptance, st.reverse_fraction)
+    smp.close()
+    prop.close()
+    return 0
+
+
 def occ(argv) -> int:
     W = int(argv[0]) if argv else 65536
     sweeps = int(argv[1]) if len(argv) > 1 else 100
@@ -70,6 +107,8 @@ def main(argv=None) -> int:
     argv = list(sys.argv[1:] if argv is None else argv)
     if argv and argv[0] == "learned":
         return learned(argv[1:])
+    if argv and argv[0] == "learned_step":
+        return learned_step(argv[1:])
     if argv and argv[0] == "occupation":
         return occ(argv[1:])
     W = int(argv[0]) if len(argv) > 0 else 16384
