@@ -28,7 +28,8 @@ ratio sums) on all host cores on a bounded sample of the same workload, with
 tau_int from a long chain of that estimator.
 ``--mixed`` gives the mixed-precision line (N = 50, dL = 0..12, 272 states),
 ``--batched`` the batched line (N = 100, dL = 1..20, 16 kappas) and
-``--evolution`` the time-evolution pipeline, each as its own JSON line.
+``--evolution`` the time-evolution pipeline, ``--occupation`` the two-state
+walker's occupations, each as its own JSON line.
 """
 from __future__ import annotations
 
@@ -753,6 +754,47 @@ def run_evolution(args, rank, local):
     print(json.dumps(line), flush=True)
 
 
+def run_occupation(args, rank, local):
+    """Orbital occupations of the two-state walker (lemc_occupation) for every
+    (L, R) row pair of one sector in one launch: N = 50, m = 3, dL = 4 (25
+    pairs), l_cutoff = m (N - 1) + 15, W = 65536 walkers split over the pairs,
+    50 burn-in + 100 measured sweeps.  Timed on the host clock around the
+    public call (allocation, launch and read-back included) after a warm-up
+    call; beside it the oracle's C restatement of the reference's walker on
+    the host cores, one pair, a bounded sample."""
+    if rank != 0:
+        return
+    import os
+
+    import laughlinedge_b200 as L
+    import torch
+    torch.cuda.set_device(local)
+    N, m, dL, W, burn, meas = 50, 3, 4, 65536, 50, 100
+    Lc = m * (N - 1) + 15
+    L.sampler.occupation(N, m, dL, Lc, W, 10, burn_in=5)
+    t0 = time.perf_counter()
+    _, acc = L.sampler.occupation(N, m, dL, Lc, W, meas, burn_in=burn)
+    t = time.perf_counter() - t0
+    rate = W * (burn + meas) / t
+    line = {"metric": "occupation_walker_sweeps_per_s", "value": rate, "unit": "walker-sweeps/s",
+            "n_gpus": 1, "higher_is_better": True, "data": "synthetic", "dtype": "f32+f64",
+            "config": {"workload": "occupation_m3_N50_dL4_W65536", "particles": N,
+                       "inverse_filling": m, "dL": dL, "l_cutoff": Lc, "walkers": W,
+                       "burn_in": burn, "sweeps": meas, "row_pairs": 25},
+            "seconds": t, "acceptance": acc}
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+        th = os.cpu_count() or 1
+        Wc, bc, mc = 64 * th, 100, 2000
+        t0 = time.perf_counter()
+        O.occupation(N, m, Wc, 0.3, 42, bc, mc, dL, 0, 0, Lc, nthreads=th)
+        tc = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": Wc * (bc + mc) / tc, "unit": "walker-sweeps/s",
+                                "cores": th, "kind": "port",
+                                "sample": f"{Wc} walkers x ({bc} + {mc}) sweeps of one row pair, {tc:.1f} s"}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -768,6 +810,8 @@ def main():
                     help="batched form N=100, dL 1..20, 16 kappas (its own JSON line)")
     ap.add_argument("--evolution", action="store_true",
                     help="time-evolution pipeline N=100, dL 0,2..16 (its own JSON line)")
+    ap.add_argument("--occupation", action="store_true",
+                    help="two-state walker occupations N=50, dL 4 (its own JSON line)")
     ap.add_argument("--graph-batch", type=int, default=4,
                     help="measured steps per CUDA-graph replay in the timed run (0: direct launches)")
     args = ap.parse_args()
@@ -781,6 +825,8 @@ def main():
             run_batched(args, rank, local)
         elif args.evolution:
             run_evolution(args, rank, local)
+        elif args.occupation:
+            run_occupation(args, rank, local)
         elif args.mixed:
             run_mixed(args, ws, rank, local)
         else:
