@@ -508,6 +508,29 @@ int gram_step(lemc_ctx* c, const float* V, const float* rec_w, int ldw, int W, i
   return s;
 }
 
+// Walker split of the contraction's jobs (tiles x splits, one CTA per SM, each
+// split a contiguous walker range): the smallest split whose jobs fill at
+// least 95 % of the SM slots of the waves they take, else the best filling one,
+// among 1..max(8, sm / tiles).  E.g. 604 tiles on 148 SMs: split 1 fills 4.08
+// of 5 waves (82 %), split 4 fills 16.3 of 17 (96 %); 20 tiles: split 7 gives
+// 140 jobs (95 %); one tile: 141 jobs.
+int wave_split(int nt, int sm, int smax) {
+  int best = 1;
+  double best_fill = 0.0;
+  const int top = std::min(smax, std::max(8, sm / std::max(1, nt)));
+  for (int s = 1; s <= top; ++s) {
+    const long jobs = long(std::max(1, nt)) * s;
+    const long waves = (jobs + sm - 1) / sm;
+    const double fill = double(jobs) / double(waves * sm);
+    if (fill >= 0.95) return s;
+    if (fill > best_fill + 1e-9) {
+      best_fill = fill;
+      best = s;
+    }
+  }
+  return best;
+}
+
 int setup_tc(lemc_ctx* c, int force_splits) {
   // Sector-aligned panels: consecutive sectors of at most 128 V rows are packed
   // into one 128-row A panel with 32-row B panels over the group's rows; a
@@ -550,9 +573,10 @@ int setup_tc(lemc_ctx* c, int force_splits) {
   c->tc_ntiles = nt;
   c->tc_maxdim = 0;
   for (int d : c->basis.sector_dim) c->tc_maxdim = std::max(c->tc_maxdim, d);
-  // one wave: at most one job per SM (unless the autotuner chose the split)
+  // one CTA per SM: the split that fills whole waves (unless the autotuner
+  // chose one)
   c->tc_splits = force_splits > 0 ? std::min(force_splits, std::max(1, c->Wpad / 128))
-                                  : std::max(1, std::min(sm / std::max(1, nt), c->Wpad / 128));
+                                  : wave_split(nt, sm, std::max(1, c->Wpad / 128));
   c->tc_tiles.clear();
   for (int sp = 0; sp < c->tc_splits; ++sp)
     for (int t = 0; t < nt; ++t)
@@ -1067,8 +1091,8 @@ static int compute_row_scales(lemc_ctx* c) {
 // Contraction autotuner (lanes_per_walker < 0, tensor-core modes): the walker
 // split of the tcgen05 jobs decides how many CTAs a launch has (tiles x split)
 // and how full its last wave is.  On a copy of the walkers, one sweep and one
-// basis build fill V; each candidate split (the one-wave rule, and the splits
-// that give 1, 2, 3 or 4 full waves of jobs) is timed over three launches
+// basis build fill V; each candidate split (the wave-filling rule, the splits
+// that give 1, 2, 3 or 4 full waves of jobs, and 1, 2, 4, 8) is timed over three launches
 // (best of two), the fastest kept.  The walkers are restored and the
 // accumulators zeroed, so the chain and its sums are those of an untuned run.
 static int autotune_gram_splits(lemc_ctx* c) {
@@ -1082,6 +1106,8 @@ static int autotune_gram_splits(lemc_ctx* c) {
     const int sp = std::min(smax, std::max(1, (waves * sm) / std::max(1, nt)));
     if (std::find(cand.begin(), cand.end(), sp) == cand.end()) cand.push_back(sp);
   }
+  for (int sp : {1, 2, 4, 8})
+    if (sp <= smax && std::find(cand.begin(), cand.end(), sp) == cand.end()) cand.push_back(sp);
   DevBuf<float2> save;
   LEMC_TRY(save.alloc(size_t(c->W) * c->N));
   LEMC_CUDA(cudaMemcpyAsync(save.p, c->pos.p, sizeof(float2) * c->W * c->N,
