@@ -511,14 +511,18 @@ int gram_step(lemc_ctx* c, const float* V, const float* rec_w, int ldw, int W, i
 // Walker split of the contraction's jobs (tiles x splits, one CTA per SM, each
 // split a contiguous walker range): the smallest split whose jobs fill at
 // least 95 % of the SM slots of the waves they take, else the best filling one,
-// among 1..max(8, sm / tiles).  E.g. 604 tiles on 148 SMs: split 1 fills 4.08
-// of 5 waves (82 %), split 4 fills 16.3 of 17 (96 %); 20 tiles: split 7 gives
-// 140 jobs (95 %); one tile: 141 jobs.
-int wave_split(int nt, int sm, int smax) {
+// among 1..max(8, sm / tiles).  A split that adds waves keeps at least 8192
+// walkers (256 K-chunks) per job, so a job's start-up and its partial-slot
+// traffic stay small against its work.  E.g. 604 tiles on 148 SMs at 65536
+// walkers: split 1 fills 4.08 of 5 waves (82 %), split 4 fills 16.3 of 17
+// (96 %); at 8192 walkers it stays 1; 20 tiles: split 7 gives 140 jobs (95 %);
+// one tile: 141 jobs.
+int wave_split(int nt, int sm, int smax, int wpad) {
   int best = 1;
   double best_fill = 0.0;
   const int top = std::min(smax, std::max(8, sm / std::max(1, nt)));
   for (int s = 1; s <= top; ++s) {
+    if (long(std::max(1, nt)) * s > sm && s > 1 && wpad / s < 8192) break;
     const long jobs = long(std::max(1, nt)) * s;
     const long waves = (jobs + sm - 1) / sm;
     const double fill = double(jobs) / double(waves * sm);
@@ -576,7 +580,7 @@ int setup_tc(lemc_ctx* c, int force_splits) {
   // one CTA per SM: the split that fills whole waves (unless the autotuner
   // chose one)
   c->tc_splits = force_splits > 0 ? std::min(force_splits, std::max(1, c->Wpad / 128))
-                                  : wave_split(nt, sm, std::max(1, c->Wpad / 128));
+                                  : wave_split(nt, sm, std::max(1, c->Wpad / 128), c->Wpad);
   c->tc_tiles.clear();
   for (int sp = 0; sp < c->tc_splits; ++sp)
     for (int t = 0; t < nt; ++t)
