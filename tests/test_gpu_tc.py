@@ -92,3 +92,23 @@ def test_tf32x3_bench_shape(lemc, oracle, cuda_ctx):
     err = _rel_err(ref, got)
     print(f"tf32x3 N=50 W=65536: max normalised error {err:.3e}")
     assert err < TOL[3]
+
+
+@pytest.mark.parametrize("N, sectors, W, splits", [
+    (200, list(range(1, 21)), 65536, 4),   # 604 tiles: 4.08 waves at split 1, 16.3 of 17 at 4
+    (200, list(range(1, 21)), 8192, 1),    # a wave-adding split keeps >= 8192 walkers per job
+    (50, list(range(13)), 65536, 7),       # 20 tiles: 140 jobs in one wave
+])
+def test_contraction_split_fills_waves(lemc, cuda_ctx, N, sectors, W, splits):
+    """The default walker split of the tcgen05 contraction (one CTA per SM on
+    the B200's 148 SMs): fill whole waves of jobs."""
+    import torch
+    if torch.cuda.get_device_properties(0).multi_processor_count != 148:
+        pytest.skip("split counts stated for 148 SMs")
+    smp = lemc.Sampler(lemc.SamplerConfig(N, 3, W, lanes_per_walker=4,
+                                          gram_mode=lemc._lib.GRAM_TF32X3), sectors)
+    smp.init_walkers()
+    smp.run(1, measure=True)
+    smp.synchronize()
+    assert smp.gram_splits() == splits
+    smp.close()
